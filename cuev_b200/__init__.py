@@ -1,0 +1,287 @@
+"""cuev_b200 — B200-native symmetric eigensolver (drop-in for cuEV's ``symm_eig_solve``).
+
+The product is ``libcuev_b200.so`` (hand-written sm_100a CUDA behind the C ABI in
+``include/cuev_b200.h``).  This module is the Python host side: it loads that library with
+ctypes and mirrors the reference's C++ interface on torch device tensors:
+
+* ``symm_eig_solve(A, n, eval, evec, stream=None, timer=None)``  — reference
+  ``cuev::symm_eig_solve<T>`` (include/cuev.h:31-33): A is overwritten, eval ascending, evec
+  columns are eigenvectors, column-major (a torch tensor ``X`` holding a column-major matrix is
+  passed as ``X`` whose memory is column-major, i.e. ``X.T`` of a row-major view).
+* ``SolverHandle`` + stage functions — reference ``SolverHandle<T>`` / ``cuev::kernels::*``
+  (include/cuda/handle.h:61-100, include/cuda/kernels.cuh:47-155).
+
+There is no CPU fallback: if the library is missing the import of any entry fails loudly.
+torch is used only for device memory and streams.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+from pathlib import Path
+
+_PKG = Path(__file__).resolve().parent
+LIB_PATH = _PKG / "libcuev_b200.so"
+
+CUEV_OK = 0
+STATUS_NAMES = {
+    0: "CUEV_OK", -1: "CUEV_ERR_INVALID", -2: "CUEV_ERR_ALLOC", -3: "CUEV_ERR_CUDA",
+    -4: "CUEV_ERR_TIMEOUT", -5: "CUEV_ERR_NONFINITE", -6: "CUEV_ERR_CONVERGENCE",
+    -7: "CUEV_ERR_UNSUPPORTED",
+}
+
+BUF_B, BUF_D, BUF_E, BUF_Y, BUF_U, BUF_TAU = range(6)
+
+
+class CuevError(RuntimeError):
+    def __init__(self, status: int, where: str, msg: str = ""):
+        self.status = status
+        super().__init__(f"{where}: {STATUS_NAMES.get(status, status)} {msg}".strip())
+
+
+class Timer(C.Structure):
+    """Same field order as the reference's cuev::SolveTimer (include/cuda/handle.h:25-37)."""
+
+    _fields_ = [(n, C.c_float) for n in (
+        "dbbr_ms", "bc_ms", "dc_ms", "bt_ms", "total_ms",
+        "bt_copyin_ms", "bt_qb_ms", "bt_qs_ms", "bt_copyout_ms")]
+
+    def as_dict(self):
+        return {n: float(getattr(self, n)) for n, _ in self._fields_}
+
+
+class Config(C.Structure):
+    _fields_ = [("nbw", C.c_int), ("nk", C.c_int)]
+
+
+class RefineInfo(C.Structure):
+    _fields_ = [("iters", C.c_int), ("resid", C.c_double), ("orth", C.c_double),
+                ("stage1_ms", C.c_float), ("refine_ms", C.c_float)]
+
+
+_VP, _I, _D, _DP, _FP = C.c_void_p, C.c_int, C.c_double, C.c_void_p, C.c_void_p
+_SIGS = {
+    "cuev_dsyevd": [_DP, _I, _DP, _DP, _VP, C.POINTER(Timer)],
+    "cuev_dsyevd_cfg": [_DP, _I, _DP, _DP, _VP, C.POINTER(Timer), C.POINTER(Config)],
+    "cuev_ssyevd": [_FP, _I, _FP, _FP, _VP, C.POINTER(Timer)],
+    "cuev_release_workspace": [],
+    "cuev_handle_create": [_I, _I, _I, _VP, C.POINTER(C.c_void_p)],
+    "cuev_handle_destroy": [_VP],
+    "cuev_handle_buffer": [_VP, _I, C.POINTER(C.c_void_p), C.POINTER(C.c_longlong)],
+    "cuev_dbbr_panel_qr": [_VP, _DP, _I, _DP, _I, _DP, _DP, _I, _I],
+    "cuev_dbbr_reduce": [_VP, _DP],
+    "cuev_dbbr_pack": [_VP, _DP, _DP],
+    "cuev_bc_chase": [_VP, _DP, _DP, _DP],
+    "cuev_tridi_dc": [_VP, _DP, _DP, _DP, _DP],
+    "cuev_bc_back": [_VP, _DP, _I],
+    "cuev_sbr_back": [_VP, _DP, _I],
+    "cuev_back_transform": [_VP, _DP, C.POINTER(Timer)],
+    "cuev_dgemm": [_VP, _I, _I, _I, _I, _I, _D, _DP, _I, _DP, _I, _D, _DP, _I],
+    "cuev_dsymm_lower": [_VP, _I, _I, _D, _DP, _I, _DP, _I, _D, _DP, _I],
+    "cuev_dsyr2k_lower": [_VP, _I, _I, _D, _DP, _I, _DP, _I, _D, _DP, _I],
+    "cuev_dsyevd_mixed": [_DP, _I, _DP, _DP, _I, _D, _VP, C.POINTER(RefineInfo)],
+    "cuev_dsyev_adjoint": [_DP, _DP, _DP, _DP, _I, _D, _DP, _VP],
+    "cuev_ssyev_adjoint": [_FP, _FP, _FP, _FP, _I, C.c_float, _FP, _VP],
+}
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load libcuev_b200.so (built by ``python -m cuev_b200.build``).  Raises if absent."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with `python -m cuev_b200.build` "
+                "(there is no CPU fallback)")
+        L = C.CDLL(str(LIB_PATH))
+        for name, args in _SIGS.items():
+            fn = getattr(L, name, None)
+            if fn is None:
+                continue
+            fn.argtypes = args
+            fn.restype = C.c_int
+        L.cuev_last_error.restype = C.c_char_p
+        L.cuev_last_error.argtypes = []
+        _lib = L
+    return _lib
+
+
+def exported_symbols() -> list[str]:
+    return [n for n in list(_SIGS) + ["cuev_last_error"] if hasattr(lib(), n)]
+
+
+def _check(status: int, where: str):
+    if status != CUEV_OK:
+        raise CuevError(status, where, lib().cuev_last_error().decode(errors="replace"))
+
+
+def _ptr(t) -> int | None:
+    if t is None:
+        return None
+    return t.data_ptr()
+
+
+def _stream(stream):
+    if stream is None:
+        import torch
+        return torch.cuda.current_stream().cuda_stream
+    if hasattr(stream, "cuda_stream"):
+        return stream.cuda_stream
+    return int(stream)
+
+
+def _need_f64(*ts):
+    import torch
+    for t in ts:
+        if t is not None:
+            if not t.is_cuda:
+                raise ValueError("cuev_b200 takes device tensors (pass .cuda())")
+            if t.dtype != torch.float64:
+                raise ValueError(f"expected float64, got {t.dtype}")
+            if not t.is_contiguous():
+                raise ValueError("tensors must be contiguous (column-major data in memory)")
+
+
+# ------------------------------------------------------------------------------------------
+# Full solves (reference include/cuev.h:31-33)
+# ------------------------------------------------------------------------------------------
+def symm_eig_solve(A, n: int, eval, evec, stream=None, timer: Timer | None = None,
+                   nbw: int = 0, nk: int = 0) -> None:
+    """In-place FP64/FP32 solve on device tensors; same argument meaning as the reference.
+
+    ``A`` holds the n x n column-major matrix (lower triangle read, overwritten), ``eval`` gets
+    the ascending eigenvalues and ``evec`` the eigenvectors as columns (column-major).
+    """
+    import torch
+    t = C.byref(timer) if timer is not None else None
+    if A.dtype == torch.float32:
+        st = lib().cuev_ssyevd(_ptr(A), n, _ptr(eval), _ptr(evec), _stream(stream), t)
+        _check(st, "cuev_ssyevd")
+        return
+    _need_f64(A, eval, evec)
+    cfg = Config(nbw, nk)
+    st = lib().cuev_dsyevd_cfg(_ptr(A), n, _ptr(eval), _ptr(evec), _stream(stream), t,
+                               C.byref(cfg))
+    _check(st, "cuev_dsyevd")
+
+
+def eigh(A_rowmajor_sym, nbw: int = 0, nk: int = 0):
+    """Convenience: eigen-decomposition of a symmetric torch matrix (returns w, V with
+    A = V diag(w) V^T, V's columns the eigenvectors).  Uses the lower triangle."""
+    import torch
+    n = A_rowmajor_sym.shape[0]
+    Acm = A_rowmajor_sym.t().contiguous().clone()  # column-major storage of A
+    w = torch.empty(n, dtype=Acm.dtype, device=Acm.device)
+    Vcm = torch.empty_like(Acm)
+    symm_eig_solve(Acm, n, w, Vcm, nbw=nbw, nk=nk)
+    return w, Vcm.t()
+
+
+def release_workspace():
+    _check(lib().cuev_release_workspace(), "cuev_release_workspace")
+
+
+# ------------------------------------------------------------------------------------------
+# Stage-level API (reference SolverHandle<T> + cuev::kernels::*)
+# ------------------------------------------------------------------------------------------
+class SolverHandle:
+    """Mirror of the reference ``SolverHandle<double>`` (handle_alloc / handle_free)."""
+
+    def __init__(self, n: int, nbw: int = 32, nk: int = 512, stream=None):
+        self.n, self.nbw, self.nk = n, nbw, nk
+        self._stream = _stream(stream)
+        h = C.c_void_p()
+        _check(lib().cuev_handle_create(n, nbw, nk, self._stream, C.byref(h)),
+               "cuev_handle_create")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            _check(lib().cuev_handle_destroy(self.h), "cuev_handle_destroy")
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def buffer(self, which: int, rows: int, cols: int):
+        """A torch view (column-major storage as a (cols, ld) row-major tensor) of a handle
+        buffer; returns (tensor, ld)."""
+        import torch
+        p = C.c_void_p()
+        ld = C.c_longlong()
+        _check(lib().cuev_handle_buffer(self.h, which, C.byref(p), C.byref(ld)),
+               "cuev_handle_buffer")
+        return _wrap_device(p.value, cols * ld.value, torch.float64).view(cols, ld.value), ld.value
+
+    # stage launchers -----------------------------------------------------------------------
+    def dbbr_panel_qr(self, A, lda, Y, ldy, tau, T, rows, b):
+        _check(lib().cuev_dbbr_panel_qr(self.h, _ptr(A), lda, _ptr(Y), ldy, _ptr(tau),
+                                         _ptr(T), rows, b), "dbbr_panel_qr")
+
+    def dbbr_reduce(self, A):
+        _check(lib().cuev_dbbr_reduce(self.h, _ptr(A)), "dbbr_reduce")
+
+    def dbbr_pack(self, A, B):
+        _check(lib().cuev_dbbr_pack(self.h, _ptr(A), _ptr(B)), "dbbr_pack")
+
+    def bc_chase(self, B, d, e):
+        _check(lib().cuev_bc_chase(self.h, _ptr(B), _ptr(d), _ptr(e)), "bc_chase")
+
+    def tridi_dc(self, d, e, eval, evec):
+        _check(lib().cuev_tridi_dc(self.h, _ptr(d), _ptr(e), _ptr(eval), _ptr(evec)),
+               "tridi_dc")
+
+    def bc_back(self, M, ldm):
+        _check(lib().cuev_bc_back(self.h, _ptr(M), ldm), "bc_back")
+
+    def sbr_back(self, M, ldm):
+        _check(lib().cuev_sbr_back(self.h, _ptr(M), ldm), "sbr_back")
+
+    def back_transform(self, evec, timer: Timer | None = None):
+        t = C.byref(timer) if timer is not None else None
+        _check(lib().cuev_back_transform(self.h, _ptr(evec), t), "back_transform")
+
+
+def _wrap_device(ptr: int, numel: int, dtype):
+    """Non-owning torch view of device memory owned by the library."""
+    import torch
+
+    class _Holder:
+        pass
+
+    h = _Holder()
+    h.__cuda_array_interface__ = {
+        "shape": (numel,), "typestr": "<f8" if dtype == torch.float64 else "<f4",
+        "data": (ptr, False), "version": 2, "strides": None,
+    }
+    return torch.as_tensor(h, device="cuda")
+
+
+# ------------------------------------------------------------------------------------------
+# GEMM entries (reference cuev::cublas wrappers)
+# ------------------------------------------------------------------------------------------
+def dgemm(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, Cm, ldc, stream=None):
+    _check(lib().cuev_dgemm(_stream(stream), int(ta), int(tb), m, n, k, alpha, _ptr(A), lda,
+                            _ptr(B), ldb, beta, _ptr(Cm), ldc), "cuev_dgemm")
+
+
+def dsymm_lower(m, n, alpha, A, lda, B, ldb, beta, Cm, ldc, stream=None):
+    _check(lib().cuev_dsymm_lower(_stream(stream), m, n, alpha, _ptr(A), lda, _ptr(B), ldb,
+                                  beta, _ptr(Cm), ldc), "cuev_dsymm_lower")
+
+
+def dsyr2k_lower(n, k, alpha, A, lda, B, ldb, beta, Cm, ldc, stream=None):
+    _check(lib().cuev_dsyr2k_lower(_stream(stream), n, k, alpha, _ptr(A), lda, _ptr(B), ldb,
+                                   beta, _ptr(Cm), ldc), "cuev_dsyr2k_lower")

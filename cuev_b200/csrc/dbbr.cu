@@ -1,0 +1,327 @@
+// Stage 1: double-blocked band reduction (DBBR), full symmetric -> band of width b.
+//
+// Algorithm (Wang et al. 2025, Algorithm 1, as run by the reference src/cuda/dbbr.cu:145-229):
+// the matrix is processed in k-column blocks; inside a block, b-column panels are factorised
+// (panel QR -> Y, T), the two-sided companion Z = P - 1/2 Y (W^T P) with P = A W, W = Y T is
+// built against the not-yet-updated trailing matrix (corrected for the block's earlier panels),
+// the next panel is updated eagerly ("green" update) and the trailing matrix once per block with
+// one SYR2K.
+//
+// What is B200-specific here:
+//  * the panel QR (reference: cuSOLVER geqrf + extract + syrk + larft, dbbr.cu:124-143) is ONE
+//    cooperative kernel: the rows x b panel is split across up to one CTA per SM and stays in
+//    shared memory for the whole factorisation; each column costs one bounded grid barrier.  The
+//    same kernel emits the unit-lower Y, tau, the block factor T and W = Y T;
+//  * every contraction runs on the FP64 DMMA GEMM (gemm.cu): SYMM reading the lower triangle,
+//    the deferral correction and the green update as two-segment-K GEMMs, the SYR2K as a
+//    lower-triangle two-segment GEMM.
+#include "solver.cuh"
+
+#include <algorithm>
+
+namespace cuev {
+namespace {
+
+constexpr int QR_THREADS = 256;
+constexpr int QR_TARGET_ROWS = 128; // rows per CTA the launcher aims for
+
+// Shared-memory layout of panel_qr_kernel<BW>:
+//   sP  [chunk][BW + 1]  this CTA's rows of the panel
+//   sGT [BW][BW]         G = V^T V below the diagonal (sGT[c][q] = G[q][c], q < c), T above
+//   sp, srow, stau [BW]  reduced dot products, broadcast row c, tau
+//   sred [QR_THREADS]    row-group partial sums
+template <int BW> size_t panel_qr_smem(int chunk) {
+    return sizeof(double) * ((size_t)chunk * (BW + 1) + BW * BW + 3 * BW + QR_THREADS);
+}
+
+template <int BW>
+__global__ void __launch_bounds__(QR_THREADS)
+    panel_qr_kernel(double *__restrict__ A, long long lda, double *__restrict__ Y, long long ldy,
+                    double *__restrict__ tau, double *__restrict__ T, double *__restrict__ W,
+                    long long ldw, int rows, int b, int chunk, double *__restrict__ part,
+                    unsigned *bar, int *status) {
+    constexpr int NRG = QR_THREADS / BW; // row groups
+    constexpr int LD = BW + 1;
+    extern __shared__ __align__(16) double sm[];
+    double *sP = sm;
+    double *sGT = sP + (size_t)chunk * LD;
+    double *sp = sGT + BW * BW;
+    double *srow = sp + BW;
+    double *stau = srow + BW;
+    double *sred = stau + BW;
+
+    const int tid = threadIdx.x;
+    const int P = gridDim.x, cta = blockIdx.x;
+    const int r0 = cta * chunk;
+    const int cnt = max(0, min(rows, r0 + chunk) - r0);
+    const int j = tid % BW, rg = tid / BW;
+
+    GridBarrier gb;
+    gb.init(bar);
+
+    // load this CTA's rows (column-major global -> row-major shared)
+    for (int idx = tid; idx < cnt * b; idx += QR_THREADS) {
+        const int r = idx % cnt, c = idx / cnt;
+        sP[r * LD + c] = A[(r0 + r) + (long long)c * lda];
+    }
+    for (int idx = tid; idx < cnt * (BW - b); idx += QR_THREADS) { // unused columns (b < BW)
+        const int r = idx % cnt, c = b + idx / cnt;
+        sP[r * LD + c] = 0.0;
+    }
+    for (int idx = tid; idx < BW * BW; idx += QR_THREADS) sGT[idx] = 0.0;
+    __syncthreads();
+
+    const int ncols = min(rows, b);
+    double *rowc = part + 2 * (size_t)P * BW; // 2 x BW broadcast slots after the partials
+
+    for (int c = 0; c < ncols; ++c) {
+        const int buf = c & 1;
+        // (1) partial dots over this CTA's rows strictly below row c:  p_j = sum x_r a_j[r]
+        double acc = 0.0;
+        const int rstart = max(0, c + 1 - r0);
+        for (int r = rstart + rg; r < cnt; r += NRG) acc += sP[r * LD + c] * sP[r * LD + j];
+        sred[tid] = acc;
+        __syncthreads();
+        if (rg == 0) {
+            double s = 0.0;
+#pragma unroll
+            for (int q = 0; q < NRG; ++q) s += sred[q * BW + j];
+            part[((size_t)buf * P + cta) * BW + j] = s;
+            if (c >= r0 && c < r0 + cnt) rowc[buf * BW + j] = sP[(c - r0) * LD + j];
+        }
+        if (!gb.sync(status, c)) return;
+
+        // (2) deterministic reduction of the P partials: NRG threads per column j
+        {
+            double s = 0.0;
+            for (int q = rg; q < P; q += NRG) s += __ldcg(&part[((size_t)buf * P + q) * BW + j]);
+            sred[tid] = s;
+            __syncthreads();
+            if (rg == 0) {
+                double tot = 0.0;
+#pragma unroll
+                for (int q = 0; q < NRG; ++q) tot += sred[q * BW + j];
+                sp[j] = tot;
+                srow[j] = __ldcg(&rowc[buf * BW + j]);
+            }
+            __syncthreads();
+        }
+
+        // (3) Householder reflector for x = A[c:, c]  (H = I - tau v v^T, v[c] = 1)
+        const double alpha = srow[c];
+        const double s2 = sp[c];
+        double beta = alpha, tauc = 0.0, scal = 0.0;
+        if (s2 > 0.0) {
+            beta = -copysign(hypot(alpha, sqrt(s2)), alpha);
+            tauc = (beta - alpha) / beta;
+            scal = 1.0 / (alpha - beta);
+        }
+        if (!isfinite(s2) || !isfinite(alpha)) {
+            if (tid == 0) dev_fail(status, CUEV_ERR_NONFINITE, c);
+        }
+        // (4) apply H to the trailing columns of own rows (j > c); v_r = scal * x_r for r > c
+        if (tauc != 0.0) {
+            const int jcol = j;
+            if (jcol > c && jcol < b) {
+                const double wj = srow[jcol] + scal * sp[jcol]; // v^T a_j
+                const double f = tauc * wj;
+                for (int r = max(0, c - r0) + rg; r < cnt; r += NRG) {
+                    const int grow = r0 + r;
+                    const double v = (grow == c) ? 1.0 : scal * sP[r * LD + c];
+                    sP[r * LD + jcol] -= f * v;
+                }
+            }
+        }
+        // G[q][c] = v_q^T v_c for q < c
+        if (tid < c) sGT[c * BW + tid] = srow[tid] + scal * sp[tid];
+        if (tid == 0) stau[c] = tauc;
+        __syncthreads();
+        // (5) store v_c (scaled) and beta in column c of own rows
+        for (int r = max(0, c - r0) + tid; r < cnt; r += QR_THREADS) {
+            const int grow = r0 + r;
+            if (grow == c)
+                sP[r * LD + c] = beta;
+            else if (grow > c)
+                sP[r * LD + c] *= scal;
+        }
+        __syncthreads();
+    }
+    for (int c = ncols + tid; c < BW; c += QR_THREADS) stau[c] = 0.0;
+    __syncthreads();
+
+    // T: T[c][c] = tau_c,  T[q][c] = -tau_c sum_{p=q}^{c-1} T[q][p] G[p][c]   (q < c)
+    // (T stored in the upper triangle of sGT, G below it)
+    for (int c = 0; c < b; ++c) {
+        if (tid < c) {
+            double s = 0.0;
+            for (int p = tid; p < c; ++p) {
+                const double tqp = (p == tid) ? stau[tid] : sGT[tid * BW + p];
+                s += tqp * sGT[c * BW + p];
+            }
+            sred[tid] = -stau[c] * s;
+        }
+        __syncthreads();
+        if (tid < c) sGT[tid * BW + c] = sred[tid];
+        __syncthreads();
+    }
+
+    // outputs: A (R above, v below), Y (unit lower trapezoid), W = Y T; CTA 0 writes T, tau
+    for (int idx = tid; idx < cnt * b; idx += QR_THREADS) {
+        const int r = idx % cnt, c = idx / cnt;
+        const int grow = r0 + r;
+        const double a = sP[r * LD + c];
+        A[grow + (long long)c * lda] = a;
+        Y[grow + (long long)c * ldy] = grow > c ? a : (grow == c ? 1.0 : 0.0);
+    }
+    if (W) {
+        for (int idx = tid; idx < cnt * b; idx += QR_THREADS) {
+            const int r = idx % cnt, c = idx / cnt;
+            const int grow = r0 + r;
+            double s = 0.0;
+            const int pmax = min(c, grow); // Y[r][p] is zero for p > grow
+            for (int p = 0; p <= pmax; ++p) {
+                const double y = grow > p ? sP[r * LD + p] : 1.0; // p == grow -> unit diagonal
+                const double tpc = (p == c) ? stau[c] : sGT[p * BW + c];
+                s += y * tpc;
+            }
+            W[grow + (long long)c * ldw] = s;
+        }
+    }
+    if (cta == 0) {
+        for (int idx = tid; idx < b * b; idx += QR_THREADS) {
+            const int q = idx % b, c = idx / b;
+            T[q + (long long)c * b] = q < c ? sGT[q * BW + c] : (q == c ? stau[c] : 0.0);
+        }
+        for (int c = tid; c < b; c += QR_THREADS) tau[c] = stau[c];
+    }
+}
+
+// Pack the lower band: B[r + j 2b] = A(j + r, j) for r <= b, 0 for b < r < 2b.
+__global__ void pack_kernel(const double *__restrict__ A, long long lda, double *__restrict__ B,
+                            int n, int b) {
+    const int ldb = 2 * b;
+    const long long total = (long long)ldb * n;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const int r = (int)(idx % ldb);
+        const int jc = (int)(idx / ldb);
+        const int i = jc + r;
+        B[idx] = (r <= b && i < n) ? A[i + (long long)jc * lda] : 0.0;
+    }
+}
+
+template <int BW> int launch_panel_qr(Workspace *ws, double *A, long long lda, double *Y,
+                                      long long ldy, double *tau, double *T, double *W,
+                                      long long ldw, int rows, int b) {
+    const int sms = num_sms();
+    int P = std::max(1, std::min(sms, div_up(rows, QR_TARGET_ROWS)));
+    int chunk = div_up(rows, P);
+    // shared memory bound: grow P (up to one CTA per SM) if the chunk does not fit
+    const size_t max_smem = 227 * 1024;
+    while (panel_qr_smem<BW>(chunk) > max_smem && P < sms) {
+        ++P;
+        chunk = div_up(rows, P);
+    }
+    if (panel_qr_smem<BW>(chunk) > max_smem) {
+        set_last_message("panel QR: panel too tall for the shared-memory resident kernel");
+        return CUEV_ERR_UNSUPPORTED;
+    }
+    if ((size_t)(2 * P + 2) * BW > ws->qr_part_elems) {
+        set_last_message("panel QR: partial-sum buffer too small");
+        return CUEV_ERR_INVALID;
+    }
+    const size_t smem = panel_qr_smem<BW>(chunk);
+    auto kern = panel_qr_kernel<BW>;
+    static bool attr = false;
+    if (!attr) {
+        CUEV_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)max_smem));
+        attr = true;
+    }
+    CUEV_TRY(cudaMemsetAsync(ws->bar, 0, 2 * sizeof(unsigned), ws->stream));
+    void *args[] = {&A, &lda, &Y, &ldy, &tau, &T, &W, &ldw, &rows, &b, &chunk,
+                    &ws->qr_part, &ws->bar, &ws->status};
+    CUEV_TRY(cudaLaunchCooperativeKernel((void *)kern, dim3(P), dim3(QR_THREADS), args, smem,
+                                         ws->stream));
+    return CUEV_OK;
+}
+
+} // namespace
+
+int panel_qr(Workspace *ws, double *A, long long lda, double *Y, long long ldy, double *tau,
+             double *T, double *W, long long ldw, int rows, int b) {
+    if (rows <= 0 || b <= 0) return CUEV_OK;
+    if (b <= 32) return launch_panel_qr<32>(ws, A, lda, Y, ldy, tau, T, W, ldw, rows, b);
+    if (b <= 64) return launch_panel_qr<64>(ws, A, lda, Y, ldy, tau, T, W, ldw, rows, b);
+    set_last_message("panel QR supports b <= 64");
+    return CUEV_ERR_INVALID;
+}
+
+int dbbr_pack(Workspace *ws, const double *A, long long lda, double *B) {
+    const long long total = 2LL * ws->b * ws->n;
+    const int blocks = (int)std::min<long long>(8LL * num_sms(), (total + 255) / 256);
+    pack_kernel<<<std::max(1, blocks), 256, 0, ws->stream>>>(A, lda, B, ws->n, ws->b);
+    CUEV_TRY(cudaGetLastError());
+    return CUEV_OK;
+}
+
+int dbbr_reduce(Workspace *ws, double *A) {
+    const int n = ws->n, b = ws->b, k = ws->k;
+    const long long ld = n;
+    double *Y = ws->Y, *Z = ws->Z, *Wp = ws->Wp;
+    CUEV_TRY(cudaMemsetAsync(Y, 0, sizeof(double) * (size_t)n * n, ws->stream));
+
+    for (int i = 0; i < n; i += k) {
+        const int kc = std::min(k, n - i);
+        int w = 0; // reflector columns accumulated in this block
+        for (int j = i; j < i + kc && j + b < n; j += b) {
+            const int rows = n - (j + b);
+            double *Apan = A + (long long)j * ld + (j + b); // A[j+b:, j:j+b]
+            double *Ypan = Y + (long long)j * ld + (j + b);
+            double *Atr = A + (long long)(j + b) * ld + (j + b);
+            double *Zcur = Z + (long long)(j - i) * ld + (j + b); // P / Z of this panel
+            double *Tpan = ws->Tp + (size_t)(j / b) * b * b;
+            double *Wpan = Wp + (j + b);
+            const double *Yblk = Y + (long long)i * ld + (j + b); // Y[j+b:, i:i+w]
+            const double *Zblk = Z + (j + b);                     // Z[j+b:, 0:w]
+
+            // panel QR -> R (in A), Y, tau, T, W = Y T
+            CUEV_CHECK_STATUS(
+                panel_qr(ws, Apan, ld, Ypan, ld, ws->tau + j, Tpan, Wpan, ld, rows, b));
+            // P = A_trail W (A_trail symmetric, lower triangle, not yet updated for this block)
+            CUEV_CHECK_STATUS(ws_symm(ws, rows, b, 1.0, Atr, ld, Wpan, ld, 0.0, Zcur, ld));
+            if (w > 0) {
+                // D1 = Z_blk^T W, D2 = Y_blk^T W ;  P -= Y_blk D1 + Z_blk D2
+                double *D1 = ws->Dwk, *D2 = ws->Dwk + (size_t)k * b;
+                CUEV_CHECK_STATUS(ws_gemm(ws, 1, 0, w, b, rows, 1.0, Zblk, ld, Wpan, ld, 0.0, D1, w));
+                CUEV_CHECK_STATUS(ws_gemm(ws, 1, 0, w, b, rows, 1.0, Yblk, ld, Wpan, ld, 0.0, D2, w));
+                CUEV_CHECK_STATUS(ws_gemm2(ws, 0, 0, rows, b, w, w, -1.0, Yblk, ld, Zblk, ld, D1, w,
+                                           D2, w, 1.0, Zcur, ld, 0));
+            }
+            // C = W^T P (b x b) ;  Z = P - 1/2 Y C
+            CUEV_CHECK_STATUS(ws_gemm(ws, 1, 0, b, b, rows, 1.0, Wpan, ld, Zcur, ld, 0.0, ws->Cwk, b));
+            CUEV_CHECK_STATUS(
+                ws_gemm(ws, 0, 0, rows, b, b, -0.5, Ypan, ld, ws->Cwk, b, 1.0, Zcur, ld));
+            w += b;
+            // green update of the next panel's columns: A[j+b:, j+b:j+2b] -= Z Yg^T + Y Zg^T
+            if (j + b < i + kc) {
+                const double *Yg = Y + (long long)i * ld + (j + b); // Y[j+b:j+2b, i:i+w]
+                const double *Zg = Z + (j + b);                     // Z[j+b:j+2b, 0:w]
+                CUEV_CHECK_STATUS(ws_gemm2(ws, 0, 1, rows, b, w, w, -1.0, Zblk, ld, Yblk, ld, Yg, ld,
+                                           Zg, ld, 1.0, Atr, ld, 0));
+            }
+        }
+        // trailing update once per block: A[i+kc:, i+kc:] -= Y Z^T + Z Y^T (lower triangle)
+        const int tn = n - (i + kc);
+        if (tn > 0 && w > 0) {
+            const double *Yt = Y + (long long)i * ld + (i + kc);
+            const double *Zt = Z + (i + kc);
+            double *At = A + (long long)(i + kc) * ld + (i + kc);
+            CUEV_CHECK_STATUS(
+                ws_gemm2(ws, 0, 1, tn, tn, w, w, -1.0, Yt, ld, Zt, ld, Zt, ld, Yt, ld, 1.0, At, ld, 1));
+        }
+    }
+    return dbbr_pack(ws, A, ld, ws->B);
+}
+
+} // namespace cuev

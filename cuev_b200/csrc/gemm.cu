@@ -1,0 +1,379 @@
+// FP64 DMMA GEMM kernels (see gemm.cuh for the contract).
+#include "gemm.cuh"
+
+#include <algorithm>
+
+namespace cuev {
+namespace {
+
+constexpr int BK = 16; // k-depth of one shared-memory stage (4 DMMA k-steps)
+constexpr int PAD = 4; // row padding (doubles): keeps fragment reads bank-conflict free
+
+template <int BM_, int BN_, int WARPS_M_, int WARPS_N_, int STAGES_> struct TileCfg {
+    static constexpr int BM = BM_, BN = BN_, WARPS_M = WARPS_M_, WARPS_N = WARPS_N_;
+    static constexpr int STAGES = STAGES_;
+    static constexpr int NT = 32 * WARPS_M * WARPS_N;
+    static constexpr int WM = BM / WARPS_M, WN = BN / WARPS_N;
+    static constexpr int MT = WM / 16, NTL = WN / 8;
+    static_assert(WM % 16 == 0 && WN % 8 == 0, "warp tile must be a multiple of the DMMA shape");
+};
+
+using CfgBig = TileCfg<128, 128, 2, 4, 3>;
+using CfgSkinny = TileCfg<128, 64, 4, 2, 4>;
+using CfgSmall = TileCfg<64, 64, 2, 2, 4>;
+
+__device__ __forceinline__ void cp_async8(double *smem, const double *gmem, bool pred) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    const int sz = pred ? 8 : 0; // src-size 0 => zero fill, nothing is read
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(sz)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N> __device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// D = A(16x4, row) * B(4x8, col) + D.  Fragment ownership (g = lane/4, t = lane%4):
+//   a0 = A[g][t], a1 = A[g+8][t];  b0 = B[t][g];  d0,d1 = D[g][2t,2t+1], d2,d3 = D[g+8][2t,2t+1]
+__device__ __forceinline__ void dmma16x8x4(double (&d)[4], double a0, double a1, double b0) {
+    asm volatile("mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, "
+                 "{%0,%1,%2,%3};\n"
+                 : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+                 : "d"(a0), "d"(a1), "d"(b0));
+}
+
+template <class C, bool TA, bool TB, bool SYMM> struct SmemLayout {
+    // "outer-contiguous" tiles are stored [k][outer] (the global matrix is contiguous along the
+    // outer index), the others [outer][k].
+    static constexpr bool A_OUTER = SYMM || !TA;
+    static constexpr bool B_OUTER = TB;
+    static constexpr int A_ELEMS = A_OUTER ? BK * (C::BM + PAD) : C::BM * (BK + PAD);
+    static constexpr int B_ELEMS = B_OUTER ? BK * (C::BN + PAD) : C::BN * (BK + PAD);
+    static constexpr int STAGE_ELEMS = A_ELEMS + B_ELEMS;
+    static constexpr size_t BYTES = (size_t)C::STAGES * STAGE_ELEMS * sizeof(double);
+};
+
+template <class C, bool TA, bool TB, bool SYMM, bool BATCHED>
+__global__ void __launch_bounds__(C::NT)
+    dgemm_kernel(const GemmArgs args_val, const GemmArgs *__restrict__ args_arr) {
+    using L = SmemLayout<C, TA, TB, SYMM>;
+    extern __shared__ __align__(16) double smem[];
+
+    const GemmArgs a = BATCHED ? args_arr[blockIdx.z] : args_val;
+    const int m = a.m, n = a.n, k1 = a.k;
+    const int Ktot = a.k + a.k2;
+    const int bm = blockIdx.x * C::BM, bn = blockIdx.y * C::BN;
+    if (bm >= m || bn >= n) return;
+    if (a.c_lower && bm + C::BM - 1 < bn) return; // tile strictly above the diagonal
+    const int split = BATCHED ? 0 : blockIdx.z;
+    const int splits = BATCHED ? 1 : a.splits;
+
+    int kbeg = 0, kend = Ktot;
+    if (splits > 1) {
+        const int kchunk = ((Ktot + splits - 1) / splits + BK - 1) / BK * BK;
+        kbeg = min(Ktot, split * kchunk);
+        kend = min(Ktot, kbeg + kchunk);
+    }
+    const int ntiles = (kend - kbeg + BK - 1) / BK;
+
+    const double *__restrict__ A = a.A;
+    const double *__restrict__ A2 = a.A2;
+    const double *__restrict__ B = a.B;
+    const double *__restrict__ B2 = a.B2;
+    const long long lda = a.lda, lda2 = a.lda2, ldb = a.ldb, ldb2 = a.ldb2;
+
+    const int tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    const int wm0 = (warp % C::WARPS_M) * C::WM;
+    const int wn0 = (warp / C::WARPS_M) * C::WN;
+
+    auto load_stage = [&](int slot, int k0) {
+        double *sA = smem + slot * L::STAGE_ELEMS;
+        double *sB = sA + L::A_ELEMS;
+        // ---- A tile: op(A)[bm .. bm+BM) x [k0 .. k0+BK)
+        const bool upper_tile = SYMM && (bm + C::BM - 1 < k0); // entirely above the diagonal
+#pragma unroll
+        for (int it = 0; it < (C::BM * BK) / C::NT; ++it) {
+            const int e = tid + it * C::NT;
+            int r, kk;
+            if (L::A_OUTER && !upper_tile) {
+                r = e % C::BM;
+                kk = e / C::BM;
+            } else {
+                kk = e % BK;
+                r = e / BK;
+            }
+            const int i = bm + r, kg = k0 + kk;
+            const bool pred = (i < m) && (kg < kend);
+            const double *src = A;
+            if (pred) {
+                if (SYMM) {
+                    src = (i >= kg) ? A + i + (long long)kg * lda : A + kg + (long long)i * lda;
+                } else if (kg < k1) {
+                    src = TA ? A + kg + (long long)i * lda : A + i + (long long)kg * lda;
+                } else {
+                    const int q = kg - k1;
+                    src = TA ? A2 + q + (long long)i * lda2 : A2 + i + (long long)q * lda2;
+                }
+            }
+            double *dst = L::A_OUTER ? sA + kk * (C::BM + PAD) + r : sA + r * (BK + PAD) + kk;
+            cp_async8(dst, src, pred);
+        }
+        // ---- B tile: op(B)[k0 .. k0+BK) x [bn .. bn+BN)
+#pragma unroll
+        for (int it = 0; it < (C::BN * BK) / C::NT; ++it) {
+            const int e = tid + it * C::NT;
+            int c, kk;
+            if (L::B_OUTER) {
+                c = e % C::BN;
+                kk = e / C::BN;
+            } else {
+                kk = e % BK;
+                c = e / BK;
+            }
+            const int j = bn + c, kg = k0 + kk;
+            const bool pred = (j < n) && (kg < kend);
+            const double *src = B;
+            if (pred) {
+                if (kg < k1) {
+                    src = TB ? B + j + (long long)kg * ldb : B + kg + (long long)j * ldb;
+                } else {
+                    const int q = kg - k1;
+                    src = TB ? B2 + j + (long long)q * ldb2 : B2 + q + (long long)j * ldb2;
+                }
+            }
+            double *dst = L::B_OUTER ? sB + kk * (C::BN + PAD) + c : sB + c * (BK + PAD) + kk;
+            cp_async8(dst, src, pred);
+        }
+    };
+
+    double acc[C::MT][C::NTL][4];
+#pragma unroll
+    for (int i = 0; i < C::MT; ++i)
+#pragma unroll
+        for (int j = 0; j < C::NTL; ++j)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.0;
+
+    // prologue
+#pragma unroll
+    for (int s = 0; s < C::STAGES - 1; ++s) {
+        if (s < ntiles) load_stage(s, kbeg + s * BK);
+        cp_async_commit();
+    }
+
+    for (int kt = 0; kt < ntiles; ++kt) {
+        cp_async_wait<C::STAGES - 2>();
+        __syncthreads();
+        {
+            const int pf = kt + C::STAGES - 1;
+            if (pf < ntiles) load_stage(pf % C::STAGES, kbeg + pf * BK);
+            cp_async_commit();
+        }
+        const double *sA = smem + (kt % C::STAGES) * L::STAGE_ELEMS;
+        const double *sB = sA + L::A_ELEMS;
+#pragma unroll
+        for (int ks = 0; ks < BK / 4; ++ks) {
+            const int kk = ks * 4 + t;
+            double af[C::MT][2], bf[C::NTL];
+#pragma unroll
+            for (int mi = 0; mi < C::MT; ++mi) {
+                const int r = wm0 + mi * 16 + g;
+                if (L::A_OUTER) {
+                    af[mi][0] = sA[kk * (C::BM + PAD) + r];
+                    af[mi][1] = sA[kk * (C::BM + PAD) + r + 8];
+                } else {
+                    af[mi][0] = sA[r * (BK + PAD) + kk];
+                    af[mi][1] = sA[(r + 8) * (BK + PAD) + kk];
+                }
+            }
+#pragma unroll
+            for (int ni = 0; ni < C::NTL; ++ni) {
+                const int c = wn0 + ni * 8 + g;
+                bf[ni] = L::B_OUTER ? sB[kk * (C::BN + PAD) + c] : sB[c * (BK + PAD) + kk];
+            }
+#pragma unroll
+            for (int mi = 0; mi < C::MT; ++mi)
+#pragma unroll
+                for (int ni = 0; ni < C::NTL; ++ni)
+                    dmma16x8x4(acc[mi][ni], af[mi][0], af[mi][1], bf[ni]);
+        }
+    }
+    cp_async_wait<0>();
+
+    // epilogue
+    const double alpha = a.alpha, beta = a.beta;
+    double *__restrict__ Cp = a.C;
+    const long long ldc = a.ldc;
+    double *__restrict__ W = (splits > 1) ? a.ws + (size_t)split * m * n : nullptr;
+#pragma unroll
+    for (int mi = 0; mi < C::MT; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < C::NTL; ++ni)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int row = bm + wm0 + mi * 16 + g + ((q & 2) ? 8 : 0);
+                const int col = bn + wn0 + ni * 8 + 2 * t + (q & 1);
+                if (row >= m || col >= n) continue;
+                if (a.c_lower && row < col) continue;
+                const double v = alpha * acc[mi][ni][q];
+                if (W) {
+                    W[row + (size_t)col * m] = v;
+                } else {
+                    double *cp = Cp + row + (long long)col * ldc;
+                    *cp = (beta != 0.0) ? v + beta * (*cp) : v;
+                }
+            }
+}
+
+// C = sum_z W_z + beta C over the (masked) m x n output.
+__global__ void splitk_reduce_kernel(int m, int n, int splits, const double *__restrict__ W,
+                                     double beta, double *__restrict__ C, long long ldc,
+                                     int c_lower) {
+    const size_t total = (size_t)m * n;
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total;
+         idx += (size_t)gridDim.x * blockDim.x) {
+        const int row = (int)(idx % m), col = (int)(idx / m);
+        if (c_lower && row < col) continue;
+        double s = 0.0;
+        for (int z = 0; z < splits; ++z) s += W[z * total + idx];
+        double *cp = C + row + (long long)col * ldc;
+        *cp = (beta != 0.0) ? s + beta * (*cp) : s;
+    }
+}
+
+template <class C, bool TA, bool TB, bool SYMM, bool BATCHED>
+int launch_cfg(const GemmArgs &a, const GemmArgs *dev_args, dim3 grid, cudaStream_t stream) {
+    using L = SmemLayout<C, TA, TB, SYMM>;
+    auto kern = dgemm_kernel<C, TA, TB, SYMM, BATCHED>;
+    static bool attr_set = false; // one attribute call per instantiation and process
+    if (!attr_set) {
+        CUEV_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)L::BYTES));
+        attr_set = true;
+    }
+    kern<<<grid, C::NT, L::BYTES, stream>>>(a, dev_args);
+    CUEV_TRY(cudaGetLastError());
+    return CUEV_OK;
+}
+
+template <class C, bool SYMM, bool BATCHED>
+int dispatch_t(const GemmArgs &a, const GemmArgs *dev_args, int ta, int tb, dim3 grid,
+               cudaStream_t stream) {
+    if (SYMM) return launch_cfg<C, false, false, true, BATCHED>(a, dev_args, grid, stream);
+    if (!ta && !tb) return launch_cfg<C, false, false, false, BATCHED>(a, dev_args, grid, stream);
+    if (!ta && tb) return launch_cfg<C, false, true, false, BATCHED>(a, dev_args, grid, stream);
+    if (ta && !tb) return launch_cfg<C, true, false, false, BATCHED>(a, dev_args, grid, stream);
+    return launch_cfg<C, true, true, false, BATCHED>(a, dev_args, grid, stream);
+}
+
+enum class Tile { Big, Skinny, Small };
+
+Tile pick_tile(int m, int n) {
+    if (m <= 64 && n <= 64) return Tile::Small;
+    if (n <= 64 || m <= 64) return Tile::Skinny;
+    return Tile::Big;
+}
+
+void tile_dims(Tile t, int &bm, int &bn) {
+    switch (t) {
+    case Tile::Big: bm = CfgBig::BM, bn = CfgBig::BN; break;
+    case Tile::Skinny: bm = CfgSkinny::BM, bn = CfgSkinny::BN; break;
+    default: bm = CfgSmall::BM, bn = CfgSmall::BN; break;
+    }
+}
+
+} // namespace
+
+int gemm_splitk_count(int m, int n, int k_total, int c_lower) {
+    if (m <= 0 || n <= 0 || k_total <= 0) return 1;
+    const Tile tl = pick_tile(m, n);
+    int bm, bn;
+    tile_dims(tl, bm, bn);
+    long long tiles = (long long)div_up(m, bm) * div_up(n, bn);
+    if (c_lower) tiles = (tiles + div_up(n, bn)) / 2;
+    const int sms = num_sms();
+    if (tiles >= sms) return 1;
+    int s = (int)std::min<long long>((2LL * sms + tiles - 1) / tiles, k_total / 256);
+    return std::max(1, std::min(s, 32));
+}
+
+size_t gemm_splitk_workspace(int m, int n, int k_total, int ta, int tb, int c_lower) {
+    (void)ta;
+    (void)tb;
+    const int s = gemm_splitk_count(m, n, k_total, c_lower);
+    return s > 1 ? (size_t)s * m * n * sizeof(double) : 0;
+}
+
+int gemm_launch(const GemmArgs &a_in, int ta, int tb, cudaStream_t stream) {
+    GemmArgs a = a_in;
+    if (a.m <= 0 || a.n <= 0) return CUEV_OK;
+    const int ktot = a.k + a.k2;
+    if (ktot <= 0 || a.alpha == 0.0) {
+        // C = beta C on the (masked) output; reuse the reduction kernel with zero splits.
+        splitk_reduce_kernel<<<std::min(4096, div_up(a.m * a.n, 256)), 256, 0, stream>>>(
+            a.m, a.n, 0, nullptr, a.beta, a.C, a.ldc, a.c_lower);
+        CUEV_TRY(cudaGetLastError());
+        return CUEV_OK;
+    }
+    if (a.splits > 1 && a.ws == nullptr) a.splits = 1;
+    if (a.splits < 1) a.splits = 1;
+    const Tile tl = pick_tile(a.m, a.n);
+    int bm, bn;
+    tile_dims(tl, bm, bn);
+    dim3 grid(div_up(a.m, bm), div_up(a.n, bn), a.splits);
+    int st;
+    switch (tl) {
+    case Tile::Big:
+        st = a.symm_a ? dispatch_t<CfgBig, true, false>(a, nullptr, 0, 0, grid, stream)
+                      : dispatch_t<CfgBig, false, false>(a, nullptr, ta, tb, grid, stream);
+        break;
+    case Tile::Skinny:
+        st = a.symm_a ? dispatch_t<CfgSkinny, true, false>(a, nullptr, 0, 0, grid, stream)
+                      : dispatch_t<CfgSkinny, false, false>(a, nullptr, ta, tb, grid, stream);
+        break;
+    default:
+        st = a.symm_a ? dispatch_t<CfgSmall, true, false>(a, nullptr, 0, 0, grid, stream)
+                      : dispatch_t<CfgSmall, false, false>(a, nullptr, ta, tb, grid, stream);
+        break;
+    }
+    if (st != CUEV_OK) return st;
+    if (a.splits > 1) {
+        const long long total = (long long)a.m * a.n;
+        const int blocks = (int)std::min<long long>(4 * num_sms(), (total + 255) / 256);
+        splitk_reduce_kernel<<<blocks, 256, 0, stream>>>(a.m, a.n, a.splits, a.ws, a.beta, a.C,
+                                                         a.ldc, a.c_lower);
+        CUEV_TRY(cudaGetLastError());
+    }
+    return CUEV_OK;
+}
+
+int gemm_batched_launch(const GemmArgs *dev_args, int count, int max_m, int max_n, int ta,
+                        int tb, cudaStream_t stream) {
+    if (count <= 0 || max_m <= 0 || max_n <= 0) return CUEV_OK;
+    const Tile tl = pick_tile(max_m, max_n);
+    int bm, bn;
+    tile_dims(tl, bm, bn);
+    GemmArgs dummy{};
+    for (int z0 = 0; z0 < count; z0 += 65535) {
+        const int cnt = std::min(65535, count - z0);
+        dim3 grid(div_up(max_m, bm), div_up(max_n, bn), cnt);
+        int st;
+        switch (tl) {
+        case Tile::Big:
+            st = dispatch_t<CfgBig, false, true>(dummy, dev_args + z0, ta, tb, grid, stream);
+            break;
+        case Tile::Skinny:
+            st = dispatch_t<CfgSkinny, false, true>(dummy, dev_args + z0, ta, tb, grid, stream);
+            break;
+        default:
+            st = dispatch_t<CfgSmall, false, true>(dummy, dev_args + z0, ta, tb, grid, stream);
+            break;
+        }
+        if (st != CUEV_OK) return st;
+    }
+    return CUEV_OK;
+}
+
+} // namespace cuev

@@ -1,0 +1,142 @@
+// Device workspace of one (n, b, k) solve: a single pool allocation carved into the buffers
+// listed in solver.cuh.  The reference allocates and frees its pool on every call
+// (src/cuda/handle.cu:16-101); here the solve entry points cache one workspace per device and
+// (n, b, k) so the steady state does no cudaMalloc.
+#include "solver.cuh"
+
+#include <algorithm>
+
+namespace cuev {
+
+namespace {
+size_t splitk_cap_bytes() { return (size_t)3 * num_sms() * 128 * 128 * sizeof(double); }
+} // namespace
+
+int workspace_create(int n, int b, int k, cudaStream_t stream, Workspace **out) {
+    *out = nullptr;
+    if (n < 0 || (b != 32 && b != 64) || k < b || k % b != 0) {
+        set_last_message("workspace: need b in {32, 64} and k a positive multiple of b");
+        return CUEV_ERR_INVALID;
+    }
+    Workspace *ws = new Workspace();
+    ws->n = n, ws->b = b, ws->k = k, ws->stream = stream;
+    CUEV_TRY(cudaGetDevice(&ws->dev));
+    const size_t N = (size_t)std::max(n, 1);
+    const size_t nn = N * N;
+    const size_t s = sizeof(double);
+    const int sms = num_sms();
+
+    struct Item {
+        void **p;
+        size_t bytes;
+    };
+    ws->qr_part_elems = (size_t)(2 * sms + 2) * 64;
+    ws->splitk_bytes = splitk_cap_bytes();
+    ws->dc_vec_elems = 24 * N + 64;
+    ws->dc_int_elems = 24 * N + 64;
+    ws->dc_gemm_args_cap = 2 * (int)(N / 8 + 8);
+    Item items[] = {
+        {(void **)&ws->Y, nn * s},
+        {(void **)&ws->U, nn * s},
+        {(void **)&ws->dc_Q2, nn * s},
+        {(void **)&ws->dc_S, nn * s},
+        {(void **)&ws->Z, N * k * s},
+        {(void **)&ws->Wp, N * b * s},
+        {(void **)&ws->Tp, (N / b + 2) * b * b * s},
+        {(void **)&ws->Tblk, (N / k + 2) * (size_t)k * k * s},
+        {(void **)&ws->tau, (N + 64) * s},
+        {(void **)&ws->Dwk, 2 * (size_t)k * b * s},
+        {(void **)&ws->Cwk, (size_t)b * b * s},
+        {(void **)&ws->B, 2 * (size_t)b * N * s},
+        {(void **)&ws->d, N * s},
+        {(void **)&ws->e, N * s},
+        {(void **)&ws->prog, N * sizeof(int)},
+        {(void **)&ws->bar, 64},
+        {(void **)&ws->status, DEV_STATUS_WORDS * sizeof(int)},
+        {(void **)&ws->qr_part, ws->qr_part_elems * s},
+        {(void **)&ws->splitk, ws->splitk_bytes},
+        {(void **)&ws->dc_vec, ws->dc_vec_elems * s},
+        {(void **)&ws->dc_int, ws->dc_int_elems * sizeof(int)},
+        {(void **)&ws->dc_gemm_args, (size_t)ws->dc_gemm_args_cap * sizeof(GemmArgs)},
+    };
+    size_t total = 0;
+    for (auto &it : items) total += align256(it.bytes);
+    if (cudaMalloc(&ws->pool, total) != cudaSuccess) {
+        cudaGetLastError();
+        delete ws;
+        char msg[160];
+        snprintf(msg, sizeof(msg), "workspace allocation of %.2f GB failed", total / 1e9);
+        set_last_message(msg);
+        return CUEV_ERR_ALLOC;
+    }
+    ws->pool_bytes = total;
+    size_t off = 0;
+    for (auto &it : items) {
+        *it.p = (char *)ws->pool + off;
+        off += align256(it.bytes);
+    }
+    CUEV_TRY(cudaMemsetAsync(ws->status, 0, DEV_STATUS_WORDS * sizeof(int), stream));
+    CUEV_TRY(cudaMemsetAsync(ws->bar, 0, 64, stream));
+    *out = ws;
+    return CUEV_OK;
+}
+
+void workspace_destroy(Workspace *ws) {
+    if (!ws) return;
+    if (ws->pool) cudaFree(ws->pool);
+    delete ws;
+}
+
+int workspace_check_status(Workspace *ws, const char *stage) {
+    int h[DEV_STATUS_WORDS] = {0};
+    CUEV_TRY(cudaMemcpyAsync(h, ws->status, sizeof(h), cudaMemcpyDeviceToHost, ws->stream));
+    CUEV_TRY(cudaStreamSynchronize(ws->stream));
+    if (h[DEV_STATUS_CODE] != 0) {
+        char msg[200];
+        snprintf(msg, sizeof(msg), "%s: device status %d (detail %d)", stage, h[DEV_STATUS_CODE],
+                 h[DEV_STATUS_WHERE]);
+        set_last_message(msg);
+        // clear for the next call
+        CUEV_TRY(cudaMemsetAsync(ws->status, 0, DEV_STATUS_WORDS * sizeof(int), ws->stream));
+        CUEV_TRY(cudaMemsetAsync(ws->bar, 0, 64, ws->stream));
+        return h[DEV_STATUS_CODE];
+    }
+    return CUEV_OK;
+}
+
+int ws_gemm2(Workspace *ws, int ta, int tb, int m, int n, int k, int k2, double alpha,
+             const double *A, long long lda, const double *A2, long long lda2, const double *B,
+             long long ldb, const double *B2, long long ldb2, double beta, double *C,
+             long long ldc, int c_lower) {
+    GemmArgs a{};
+    a.m = m, a.n = n, a.k = k, a.k2 = k2;
+    a.A = A, a.lda = lda, a.A2 = A2, a.lda2 = lda2;
+    a.B = B, a.ldb = ldb, a.B2 = B2, a.ldb2 = ldb2;
+    a.C = C, a.ldc = ldc, a.alpha = alpha, a.beta = beta, a.c_lower = c_lower;
+    int splits = gemm_splitk_count(m, n, k + k2, c_lower);
+    while (splits > 1 && (size_t)splits * m * n * sizeof(double) > ws->splitk_bytes) --splits;
+    a.splits = splits;
+    a.ws = splits > 1 ? ws->splitk : nullptr;
+    return gemm_launch(a, ta, tb, ws->stream);
+}
+
+int ws_gemm(Workspace *ws, int ta, int tb, int m, int n, int k, double alpha, const double *A,
+            long long lda, const double *B, long long ldb, double beta, double *C, long long ldc) {
+    return ws_gemm2(ws, ta, tb, m, n, k, 0, alpha, A, lda, nullptr, 0, B, ldb, nullptr, 0, beta, C,
+                    ldc, 0);
+}
+
+int ws_symm(Workspace *ws, int m, int n, double alpha, const double *A, long long lda,
+            const double *B, long long ldb, double beta, double *C, long long ldc) {
+    GemmArgs a{};
+    a.m = m, a.n = n, a.k = m;
+    a.A = A, a.lda = lda, a.B = B, a.ldb = ldb, a.C = C, a.ldc = ldc;
+    a.alpha = alpha, a.beta = beta, a.symm_a = 1;
+    int splits = gemm_splitk_count(m, n, m, 0);
+    while (splits > 1 && (size_t)splits * m * n * sizeof(double) > ws->splitk_bytes) --splits;
+    a.splits = splits;
+    a.ws = splits > 1 ? ws->splitk : nullptr;
+    return gemm_launch(a, 0, 0, ws->stream);
+}
+
+} // namespace cuev

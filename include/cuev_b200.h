@@ -1,0 +1,159 @@
+/*
+ * cuev_b200.h — C ABI of the B200-native cuEV symmetric eigensolver (libcuev_b200.so).
+ *
+ * Drop-in target: cuEV's `cuev::symm_eig_solve<T>(T *A, int n, T *eval, T *evec,
+ * cudaStream_t stream, SolveTimer *timer)` (reference include/cuev.h:31-33).  The C++ template
+ * with that exact signature and mangled name is declared in include/cuev.h and forwards here.
+ *
+ * Conventions (same as the reference, README.md:10-12, CONVENTIONS.md:126):
+ *   - all matrices column-major, leading dimension n unless an `ld` argument says otherwise;
+ *   - only the LOWER triangle of A is read (reference src/cuda/dbbr.cu:175,222) and A is
+ *     overwritten;
+ *   - eval ascending, evec column j = eigenvector of eval[j] (sign unspecified);
+ *   - every pointer argument is a device pointer unless the name ends in `_host`;
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).  Solves are
+ *     host-blocking like the reference (src/cuda/solver.cu:59); stage entries are asynchronous.
+ *
+ * Errors: every entry returns a cuev_status.  The reference prints and calls exit(1)
+ * (include/common.h:9-34); here the C++ shim in include/cuev.h keeps that behaviour while the C
+ * entries return the code.  cuev_last_error() gives a human-readable message.
+ */
+#ifndef CUEV_B200_H
+#define CUEV_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum cuev_status {
+    CUEV_OK = 0,
+    CUEV_ERR_INVALID = -1,     /* bad argument (n < 0, null pointer, unsupported b/k, ...) */
+    CUEV_ERR_ALLOC = -2,       /* device workspace allocation failed */
+    CUEV_ERR_CUDA = -3,        /* a CUDA runtime call failed */
+    CUEV_ERR_TIMEOUT = -4,     /* a bounded device wait gave up (wavefront / grid barrier) */
+    CUEV_ERR_NONFINITE = -5,   /* NaN or Inf met in the input */
+    CUEV_ERR_CONVERGENCE = -6, /* an iteration (leaf QL, secular solver, refinement) failed */
+    CUEV_ERR_UNSUPPORTED = -7  /* form not built for this dtype / size */
+} cuev_status;
+
+/* Per-stage timings; same fields, order and meaning as cuev::SolveTimer
+ * (reference include/cuda/handle.h:25-37). */
+typedef struct cuev_timer {
+    float dbbr_ms;       /* full -> band (DBBR, incl. pack) */
+    float bc_ms;         /* band -> tridiagonal (bulge chasing) */
+    float dc_ms;         /* tridiagonal divide and conquer (on the GPU here) */
+    float bt_ms;         /* back-transform evec = Q_s * Q_b * Q_d */
+    float total_ms;      /* whole-solve wall clock */
+    float bt_copyin_ms;  /* kept for layout compatibility (no copy-in is needed here: 0) */
+    float bt_qb_ms;      /* BC-Back  M <- Q_b * M */
+    float bt_qs_ms;      /* SBR-Back M <- Q_s * M */
+    float bt_copyout_ms; /* kept for layout compatibility (0) */
+} cuev_timer;
+
+/* Blocking parameters.  0 selects the default for the size.  b in {32, 64}; k a multiple of b. */
+typedef struct cuev_config {
+    int nbw; /* band width b (reference hard-codes 32, src/cuda/solver.cu:33) */
+    int nk;  /* DBBR outer block k (reference hard-codes 512) */
+} cuev_config;
+
+/* ---------------------------------------------------------------------------------------------
+ * Full solves
+ * ------------------------------------------------------------------------------------------ */
+
+/* Plain FP64 solve.  Replaces cuev::symm_eig_solve<double> (reference src/cuda/solver.cu:25-73,
+ * instantiated at :79).  timer may be NULL. */
+int cuev_dsyevd(double *A, int n, double *eval, double *evec, void *stream, cuev_timer *timer);
+
+/* Same with explicit blocking (reference: handle_alloc(n, nbw, nk, stream),
+ * src/cuda/handle.cu:16). cfg may be NULL. */
+int cuev_dsyevd_cfg(double *A, int n, double *eval, double *evec, void *stream, cuev_timer *timer,
+                    const cuev_config *cfg);
+
+/* FP32 interface.  Replaces cuev::symm_eig_solve<float> (reference src/cuda/solver.cu:78).
+ * The float input is widened and solved by the FP64 pipeline, then rounded back. */
+int cuev_ssyevd(float *A, int n, float *eval, float *evec, void *stream, cuev_timer *timer);
+
+/* Release the cached device workspace (the solves keep one pool per (n, b, k) between calls). */
+int cuev_release_workspace(void);
+
+/* Message for the last failing call on this host thread ("" if none). */
+const char *cuev_last_error(void);
+
+/* ---------------------------------------------------------------------------------------------
+ * Stage-level API used by the stage tests.  Mirrors the reference's SolverHandle<T> and
+ * cuev::kernels::* launchers (include/cuda/handle.h:61-100, include/cuda/kernels.cuh:47-155).
+ * A handle owns the workspace for one (n, b, k); every stage call is enqueued on the handle's
+ * stream and returns without synchronising.
+ * ------------------------------------------------------------------------------------------ */
+typedef struct cuev_handle_s *cuev_handle;
+
+/* Replaces cuev::handle_alloc<double> (reference src/cuda/handle.cu:16-94). */
+int cuev_handle_create(int n, int nbw, int nk, void *stream, cuev_handle *out);
+/* Replaces cuev::handle_free<double> (reference src/cuda/handle.cu:96-101). */
+int cuev_handle_destroy(cuev_handle h);
+
+/* Device buffers owned by the handle (what the reference tests read from ws.B, ws.d, ...). */
+typedef enum cuev_buffer {
+    CUEV_BUF_B = 0, /* packed band, 2b x n, ld 2b (reference ws.B) */
+    CUEV_BUF_D = 1, /* tridiagonal diagonal, n */
+    CUEV_BUF_E = 2, /* tridiagonal sub-diagonal, n-1 */
+    CUEV_BUF_Y = 3, /* DBBR reflectors, n x n, ld n (reference ws.Y) */
+    CUEV_BUF_U = 4, /* bulge-chasing reflectors, column s = sweep s, ld n (reference ws.U) */
+    CUEV_BUF_TAU = 5 /* DBBR Householder scalars, n (one per reflector column) */
+} cuev_buffer;
+int cuev_handle_buffer(cuev_handle h, int which, void **ptr, long long *ld);
+
+/* Panel QR of a rows x b panel (b <= 64): R in the upper triangle of A, unit lower-trapezoidal
+ * reflectors in Y (ld ldy), scalars in tau (b), block factor T (b x b, ld b, upper) with
+ * H_0...H_{b-1} = I - Y T Y^T.  Replaces kernels::dbbr_panel_qr (reference src/cuda/dbbr.cu:124-143:
+ * cuSOLVER geqrf + extract + larft). */
+int cuev_dbbr_panel_qr(cuev_handle h, double *A, int lda, double *Y, int ldy, double *tau,
+                       double *T, int rows, int b);
+
+/* Full-to-band reduction of the lower triangle of A (ld n) in place; the band is also packed
+ * into the handle's B.  Replaces kernels::dbbr_reduce (reference src/cuda/dbbr.cu:145-229). */
+int cuev_dbbr_reduce(cuev_handle h, double *A);
+
+/* Pack the lower band of A (ld n) into B (2b x n).  Replaces kernels::dbbr_pack
+ * (reference src/cuda/dbbr.cu:116-122). */
+int cuev_dbbr_pack(cuev_handle h, const double *A, double *B);
+
+/* Band -> tridiagonal (d, e); reflectors kept in the handle's U.  Replaces kernels::bc_chase
+ * (reference src/cuda/bulge.cu:231-247). */
+int cuev_bc_chase(cuev_handle h, double *B, double *d, double *e);
+
+/* Tridiagonal divide and conquer on the GPU: eval ascending, evec = eigenvectors of the
+ * tridiagonal (n x n, ld n).  d and e are not modified.  Replaces kernels::tridi_dc (reference
+ * src/cuda/tridi.cu:425-452, a host LAPACK D&C). */
+int cuev_tridi_dc(cuev_handle h, const double *d, const double *e, double *eval, double *evec);
+
+/* M <- Q_b M (n x n, ld ldm).  Replaces kernels::bc_back (reference src/cuda/backtransform.cu:183-207). */
+int cuev_bc_back(cuev_handle h, double *M, int ldm);
+
+/* M <- Q_s M (n x n, ld ldm).  Replaces kernels::sbr_back (reference src/cuda/backtransform.cu:210-230). */
+int cuev_sbr_back(cuev_handle h, double *M, int ldm);
+
+/* evec <- Q_s Q_b evec.  Replaces kernels::back_transform (reference src/cuda/backtransform.cu:232-275). */
+int cuev_back_transform(cuev_handle h, double *evec, cuev_timer *timer);
+
+/* FP64 tensor-core GEMM used by every stage: C = alpha op(A) op(B) + beta C (column-major).
+ * ta/tb: 0 = N, 1 = T.  Replaces the reference's cuev::cublas::gemm wrapper
+ * (src/cuda/cublas.cu:15-26). */
+int cuev_dgemm(void *stream, int ta, int tb, int m, int n, int k, double alpha, const double *A,
+               int lda, const double *B, int ldb, double beta, double *C, int ldc);
+
+/* C = alpha A B + beta C with A symmetric (m x m, lower triangle read).  Replaces
+ * cuev::cublas::symm(LEFT, LOWER) (reference src/cuda/cublas.cu:28-37). */
+int cuev_dsymm_lower(void *stream, int m, int n, double alpha, const double *A, int lda,
+                     const double *B, int ldb, double beta, double *C, int ldc);
+
+/* Lower triangle of C = alpha (A B^T + B A^T) + beta C, C n x n, A and B n x k.  Replaces
+ * cuev::cublas::syr2k(LOWER, N) (reference src/cuda/cublas.cu:48-56). */
+int cuev_dsyr2k_lower(void *stream, int n, int k, double alpha, const double *A, int lda,
+                      const double *B, int ldb, double beta, double *C, int ldc);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CUEV_B200_H */
