@@ -1,0 +1,364 @@
+// C ABI (include/cuev_b200.h) and the C++ drop-in shim (include/cuev.h).
+//
+// Full solves keep one cached workspace per device and (n, b, k) so repeated calls do not
+// allocate; a call that finds the cached workspace busy (another host thread) allocates its own,
+// which keeps the reference's reentrancy (its handle is per call, src/cuda/solver.cu:33,72).
+#include "solver.cuh"
+
+#include "../../include/cuev.h"
+
+#include <chrono>
+#include <cstdlib>
+#include <mutex>
+
+struct cuev_handle_s {
+    cuev::Workspace *ws;
+};
+
+namespace cuev {
+namespace {
+
+struct CachedWs {
+    Workspace *ws = nullptr;
+    bool busy = false;
+};
+std::mutex g_cache_mu;
+CachedWs g_cache[64];
+
+int default_b(int n) { return n >= 4096 ? 64 : 32; }
+int default_k(int n, int b) {
+    (void)n;
+    return b == 64 ? 512 : 256;
+}
+
+int acquire_ws(int n, int b, int k, cudaStream_t stream, Workspace **out, bool *cached) {
+    int dev = 0;
+    CUEV_TRY(cudaGetDevice(&dev));
+    *cached = false;
+    {
+        std::lock_guard<std::mutex> lk(g_cache_mu);
+        CachedWs &c = g_cache[dev & 63];
+        if (!c.busy) {
+            if (c.ws && (c.ws->n != n || c.ws->b != b || c.ws->k != k)) {
+                cudaDeviceSynchronize();
+                workspace_destroy(c.ws);
+                c.ws = nullptr;
+            }
+            if (!c.ws) CUEV_CHECK_STATUS(workspace_create(n, b, k, stream, &c.ws));
+            c.busy = true;
+            c.ws->stream = stream;
+            *out = c.ws;
+            *cached = true;
+            return CUEV_OK;
+        }
+    }
+    return workspace_create(n, b, k, stream, out);
+}
+
+void release_ws(Workspace *ws, bool cached) {
+    if (cached) {
+        std::lock_guard<std::mutex> lk(g_cache_mu);
+        for (auto &c : g_cache)
+            if (c.ws == ws) c.busy = false;
+    } else {
+        workspace_destroy(ws);
+    }
+}
+
+// Non-finite scan of the lower triangle.
+__global__ void nonfinite_scan_kernel(const double *__restrict__ A, int n, long long lda,
+                                      int *status) {
+    const long long total = (long long)n * n;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(idx % n), j = (int)(idx / n);
+        if (i >= j && !isfinite(A[i + (long long)j * lda])) {
+            dev_fail(status, CUEV_ERR_NONFINITE, j);
+            return;
+        }
+    }
+}
+
+__global__ void small_solve_kernel(const double *A, double *eval, double *evec) {
+    eval[0] = A[0];
+    evec[0] = 1.0;
+}
+
+struct EventSet {
+    cudaEvent_t e[6] = {};
+    bool on = false;
+    int create() {
+        for (auto &x : e) CUEV_TRY(cudaEventCreate(&x));
+        on = true;
+        return CUEV_OK;
+    }
+    ~EventSet() {
+        if (on)
+            for (auto &x : e) cudaEventDestroy(x);
+    }
+};
+
+int solve_d(double *A, int n, double *eval, double *evec, cudaStream_t stream, cuev_timer *timer,
+            const cuev_config *cfg) {
+    if (n < 0) return CUEV_ERR_INVALID;
+    if (n == 0) return CUEV_OK;
+    if (!A || !eval || !evec) return CUEV_ERR_INVALID;
+    auto wall0 = std::chrono::high_resolution_clock::now();
+    if (n == 1) {
+        small_solve_kernel<<<1, 1, 0, stream>>>(A, eval, evec);
+        CUEV_TRY(cudaGetLastError());
+        CUEV_TRY(cudaStreamSynchronize(stream));
+        if (timer) *timer = cuev_timer{};
+        return CUEV_OK;
+    }
+    int b = (cfg && cfg->nbw) ? cfg->nbw : default_b(n);
+    int k = (cfg && cfg->nk) ? cfg->nk : default_k(n, b);
+    Workspace *ws = nullptr;
+    bool cached = false;
+    CUEV_CHECK_STATUS(acquire_ws(n, b, k, stream, &ws, &cached));
+    struct Guard {
+        Workspace *ws;
+        bool cached;
+        ~Guard() { release_ws(ws, cached); }
+    } guard{ws, cached};
+
+    EventSet ev;
+    if (timer) CUEV_CHECK_STATUS(ev.create());
+    auto rec = [&](int i) -> int {
+        if (timer) CUEV_TRY(cudaEventRecord(ev.e[i], stream));
+        return CUEV_OK;
+    };
+    nonfinite_scan_kernel<<<4 * num_sms(), 256, 0, stream>>>(A, n, n, ws->status);
+    CUEV_TRY(cudaGetLastError());
+    CUEV_CHECK_STATUS(workspace_check_status(ws, "input scan"));
+
+    CUEV_CHECK_STATUS(rec(0));
+    CUEV_CHECK_STATUS(dbbr_reduce(ws, A));
+    CUEV_CHECK_STATUS(rec(1));
+    CUEV_CHECK_STATUS(bc_chase(ws, ws->B, ws->d, ws->e));
+    CUEV_CHECK_STATUS(rec(2));
+    CUEV_CHECK_STATUS(tridi_dc(ws, ws->d, ws->e, eval, evec));
+    CUEV_CHECK_STATUS(rec(3));
+    CUEV_CHECK_STATUS(bc_back(ws, evec, n));
+    CUEV_CHECK_STATUS(rec(4));
+    CUEV_CHECK_STATUS(sbr_back(ws, evec, n));
+    CUEV_CHECK_STATUS(rec(5));
+    CUEV_CHECK_STATUS(workspace_check_status(ws, "solve"));
+    auto wall1 = std::chrono::high_resolution_clock::now();
+    if (timer) {
+        float t[5];
+        for (int i = 0; i < 5; ++i) CUEV_TRY(cudaEventElapsedTime(&t[i], ev.e[i], ev.e[i + 1]));
+        *timer = cuev_timer{};
+        timer->dbbr_ms = t[0];
+        timer->bc_ms = t[1];
+        timer->dc_ms = t[2];
+        timer->bt_qb_ms = t[3];
+        timer->bt_qs_ms = t[4];
+        timer->bt_ms = t[3] + t[4];
+        timer->total_ms = std::chrono::duration<float, std::milli>(wall1 - wall0).count();
+    }
+    return CUEV_OK;
+}
+
+__global__ void widen_kernel(const float *__restrict__ s, double *__restrict__ d, long long cnt) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < cnt;
+         i += (long long)gridDim.x * blockDim.x)
+        d[i] = (double)s[i];
+}
+__global__ void narrow_kernel(const double *__restrict__ s, float *__restrict__ d, long long cnt) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < cnt;
+         i += (long long)gridDim.x * blockDim.x)
+        d[i] = (float)s[i];
+}
+
+} // namespace
+} // namespace cuev
+
+using namespace cuev;
+
+extern "C" int cuev_dsyevd_cfg(double *A, int n, double *eval, double *evec, void *stream,
+                               cuev_timer *timer, const cuev_config *cfg) {
+    return solve_d(A, n, eval, evec, (cudaStream_t)stream, timer, cfg);
+}
+
+extern "C" int cuev_dsyevd(double *A, int n, double *eval, double *evec, void *stream,
+                           cuev_timer *timer) {
+    return solve_d(A, n, eval, evec, (cudaStream_t)stream, timer, nullptr);
+}
+
+extern "C" int cuev_ssyevd(float *A, int n, float *eval, float *evec, void *stream,
+                           cuev_timer *timer) {
+    if (n < 0) return CUEV_ERR_INVALID;
+    if (n == 0) return CUEV_OK;
+    if (!A || !eval || !evec) return CUEV_ERR_INVALID;
+    cudaStream_t st = (cudaStream_t)stream;
+    const long long nn = (long long)n * n;
+    double *buf = nullptr;
+    if (cudaMallocAsync((void **)&buf, sizeof(double) * (2 * nn + n), st) != cudaSuccess) {
+        cudaGetLastError();
+        set_last_message("FP32 entry: widening buffer allocation failed");
+        return CUEV_ERR_ALLOC;
+    }
+    double *A64 = buf, *V64 = buf + nn, *w64 = buf + 2 * nn;
+    const int blocks = 4 * num_sms();
+    widen_kernel<<<blocks, 256, 0, st>>>(A, A64, nn);
+    int s = solve_d(A64, n, w64, V64, st, timer, nullptr);
+    if (s == CUEV_OK) {
+        narrow_kernel<<<blocks, 256, 0, st>>>(V64, evec, nn);
+        narrow_kernel<<<1, 256, 0, st>>>(w64, eval, n);
+        narrow_kernel<<<blocks, 256, 0, st>>>(A64, A, nn); // A is clobbered like the reference's
+    }
+    cudaFreeAsync(buf, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess && s == CUEV_OK) s = CUEV_ERR_CUDA;
+    return s;
+}
+
+extern "C" int cuev_release_workspace(void) {
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    for (auto &c : g_cache) {
+        if (c.ws && !c.busy) {
+            cudaDeviceSynchronize();
+            workspace_destroy(c.ws);
+            c.ws = nullptr;
+        }
+    }
+    return CUEV_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Stage-level API
+// ---------------------------------------------------------------------------------------------
+extern "C" int cuev_handle_create(int n, int nbw, int nk, void *stream, cuev_handle *out) {
+    if (!out) return CUEV_ERR_INVALID;
+    *out = nullptr;
+    Workspace *ws = nullptr;
+    CUEV_CHECK_STATUS(workspace_create(n, nbw, nk, (cudaStream_t)stream, &ws));
+    *out = new cuev_handle_s{ws};
+    return CUEV_OK;
+}
+
+extern "C" int cuev_handle_destroy(cuev_handle h) {
+    if (!h) return CUEV_ERR_INVALID;
+    if (h->ws) {
+        cudaStreamSynchronize(h->ws->stream);
+        workspace_destroy(h->ws);
+    }
+    delete h;
+    return CUEV_OK;
+}
+
+extern "C" int cuev_handle_buffer(cuev_handle h, int which, void **ptr, long long *ld) {
+    if (!h || !h->ws || !ptr || !ld) return CUEV_ERR_INVALID;
+    Workspace *ws = h->ws;
+    switch (which) {
+    case CUEV_BUF_B: *ptr = ws->B, *ld = 2LL * ws->b; break;
+    case CUEV_BUF_D: *ptr = ws->d, *ld = ws->n; break;
+    case CUEV_BUF_E: *ptr = ws->e, *ld = ws->n; break;
+    case CUEV_BUF_Y: *ptr = ws->Y, *ld = ws->n; break;
+    case CUEV_BUF_U: *ptr = ws->U, *ld = ws->n; break;
+    case CUEV_BUF_TAU: *ptr = ws->tau, *ld = ws->n; break;
+    default: return CUEV_ERR_INVALID;
+    }
+    return CUEV_OK;
+}
+
+#define HCHECK(h)                                                                                  \
+    do {                                                                                           \
+        if (!(h) || !(h)->ws) return CUEV_ERR_INVALID;                                             \
+    } while (0)
+
+extern "C" int cuev_dbbr_panel_qr(cuev_handle h, double *A, int lda, double *Y, int ldy,
+                                  double *tau, double *T, int rows, int b) {
+    HCHECK(h);
+    if (rows < 0 || b <= 0 || b > 64 || lda < rows || ldy < rows || !A || !Y || !tau || !T)
+        return CUEV_ERR_INVALID;
+    CUEV_CHECK_STATUS(panel_qr(h->ws, A, lda, Y, ldy, tau, T, nullptr, 0, rows, b));
+    return workspace_check_status(h->ws, "dbbr_panel_qr");
+}
+
+extern "C" int cuev_dbbr_reduce(cuev_handle h, double *A) {
+    HCHECK(h);
+    if (!A) return CUEV_ERR_INVALID;
+    CUEV_CHECK_STATUS(dbbr_reduce(h->ws, A));
+    return workspace_check_status(h->ws, "dbbr_reduce");
+}
+
+extern "C" int cuev_dbbr_pack(cuev_handle h, const double *A, double *B) {
+    HCHECK(h);
+    if (!A || !B) return CUEV_ERR_INVALID;
+    return dbbr_pack(h->ws, A, h->ws->n, B);
+}
+
+extern "C" int cuev_bc_chase(cuev_handle h, double *B, double *d, double *e) {
+    HCHECK(h);
+    if (!B || !d || !e) return CUEV_ERR_INVALID;
+    CUEV_CHECK_STATUS(bc_chase(h->ws, B, d, e));
+    return workspace_check_status(h->ws, "bc_chase");
+}
+
+extern "C" int cuev_tridi_dc(cuev_handle h, const double *d, const double *e, double *eval,
+                             double *evec) {
+    HCHECK(h);
+    if (!d || !e || !eval || !evec) return CUEV_ERR_INVALID;
+    CUEV_CHECK_STATUS(tridi_dc(h->ws, d, e, eval, evec));
+    return workspace_check_status(h->ws, "tridi_dc");
+}
+
+extern "C" int cuev_bc_back(cuev_handle h, double *M, int ldm) {
+    HCHECK(h);
+    if (!M || ldm < h->ws->n) return CUEV_ERR_INVALID;
+    return bc_back(h->ws, M, ldm);
+}
+
+extern "C" int cuev_sbr_back(cuev_handle h, double *M, int ldm) {
+    HCHECK(h);
+    if (!M || ldm < h->ws->n) return CUEV_ERR_INVALID;
+    return sbr_back(h->ws, M, ldm);
+}
+
+extern "C" int cuev_back_transform(cuev_handle h, double *evec, cuev_timer *timer) {
+    HCHECK(h);
+    if (!evec) return CUEV_ERR_INVALID;
+    Workspace *ws = h->ws;
+    EventSet ev;
+    if (timer) CUEV_CHECK_STATUS(ev.create());
+    if (timer) CUEV_TRY(cudaEventRecord(ev.e[0], ws->stream));
+    CUEV_CHECK_STATUS(bc_back(ws, evec, ws->n));
+    if (timer) CUEV_TRY(cudaEventRecord(ev.e[1], ws->stream));
+    CUEV_CHECK_STATUS(sbr_back(ws, evec, ws->n));
+    if (timer) {
+        CUEV_TRY(cudaEventRecord(ev.e[2], ws->stream));
+        CUEV_TRY(cudaEventSynchronize(ev.e[2]));
+        *timer = cuev_timer{};
+        CUEV_TRY(cudaEventElapsedTime(&timer->bt_qb_ms, ev.e[0], ev.e[1]));
+        CUEV_TRY(cudaEventElapsedTime(&timer->bt_qs_ms, ev.e[1], ev.e[2]));
+        timer->bt_ms = timer->bt_qb_ms + timer->bt_qs_ms;
+    }
+    return CUEV_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// C++ drop-in: cuev::symm_eig_solve<T> with the reference's signature and mangled names.
+// ---------------------------------------------------------------------------------------------
+static_assert(sizeof(cuev::SolveTimer) == sizeof(cuev_timer), "SolveTimer layout");
+
+namespace cuev {
+template <>
+void symm_eig_solve<double>(double *A, int n, double *eval, double *evec, cudaStream_t stream,
+                            SolveTimer *timer) {
+    const int st = cuev_dsyevd(A, n, eval, evec, stream, reinterpret_cast<cuev_timer *>(timer));
+    if (st != CUEV_OK) {
+        fprintf(stderr, "cuev::symm_eig_solve<double> failed: %d (%s)\n", st, cuev_last_error());
+        exit(1);
+    }
+}
+template <>
+void symm_eig_solve<float>(float *A, int n, float *eval, float *evec, cudaStream_t stream,
+                           SolveTimer *timer) {
+    const int st = cuev_ssyevd(A, n, eval, evec, stream, reinterpret_cast<cuev_timer *>(timer));
+    if (st != CUEV_OK) {
+        fprintf(stderr, "cuev::symm_eig_solve<float> failed: %d (%s)\n", st, cuev_last_error());
+        exit(1);
+    }
+}
+} // namespace cuev

@@ -265,6 +265,33 @@ int dbbr_pack(Workspace *ws, const double *A, long long lda, double *B) {
     return CUEV_OK;
 }
 
+namespace {
+int build_block_t(Workspace *ws, int i, int w) {
+    const int n = ws->n, b = ws->b, k = ws->k;
+    const long long ld = n;
+    const int rows = n - (i + b);
+    double *Tb = ws->Tblk + (size_t)(i / k) * k * k;
+    const double *Yb = ws->Y + (long long)i * ld + (i + b);
+    CUEV_TRY(cudaMemsetAsync(Tb, 0, sizeof(double) * (size_t)k * k, ws->stream));
+    // G = Y_blk^T Y_blk  (w x w, ld k)
+    CUEV_CHECK_STATUS(ws_gemm(ws, 1, 0, w, w, rows, 1.0, Yb, ld, Yb, ld, 0.0, ws->Gblk, k));
+    for (int q = 0; q * b < w; ++q) {
+        const int qb = q * b;
+        const double *Tq = ws->Tp + (size_t)((i + qb) / b) * b * b;
+        CUEV_TRY(cudaMemcpy2DAsync(Tb + qb + (size_t)qb * k, k * sizeof(double), Tq,
+                                   b * sizeof(double), b * sizeof(double), b,
+                                   cudaMemcpyDeviceToDevice, ws->stream));
+        if (q == 0) continue;
+        double *X = ws->Dwk; // qb x b
+        CUEV_CHECK_STATUS(ws_gemm(ws, 0, 0, qb, b, b, 1.0, ws->Gblk + (size_t)qb * k, k, Tq, b,
+                                  0.0, X, qb));
+        CUEV_CHECK_STATUS(ws_gemm(ws, 0, 0, qb, b, qb, -1.0, Tb, k, X, qb, 0.0,
+                                  Tb + (size_t)qb * k, k));
+    }
+    return CUEV_OK;
+}
+} // namespace
+
 int dbbr_reduce(Workspace *ws, double *A) {
     const int n = ws->n, b = ws->b, k = ws->k;
     const long long ld = n;
@@ -311,6 +338,10 @@ int dbbr_reduce(Workspace *ws, double *A) {
                                            Zg, ld, 1.0, Atr, ld, 0));
             }
         }
+        // aggregated WY factor of the block for the back-transform:
+        //   prod_q (I - Y_q T_q Y_q^T) = I - Y_blk T_blk Y_blk^T,
+        //   T_blk[0:q, q] = -T_blk[0:q, 0:q] (Y_blk[:, 0:q]^T Y_q) T_q   (compact-WY merge)
+        if (w > 0) CUEV_CHECK_STATUS(build_block_t(ws, i, w));
         // trailing update once per block: A[i+kc:, i+kc:] -= Y Z^T + Z Y^T (lower triangle)
         const int tn = n - (i + kc);
         if (tn > 0 && w > 0) {

@@ -25,7 +25,7 @@ struct Workspace {
     cudaStream_t stream = nullptr;
 
     double *Y = nullptr, *Z = nullptr, *Wp = nullptr, *Tp = nullptr, *Tblk = nullptr;
-    double *tau = nullptr, *Dwk = nullptr, *Cwk = nullptr;
+    double *tau = nullptr, *Dwk = nullptr, *Cwk = nullptr, *Gblk = nullptr;
     double *B = nullptr, *U = nullptr, *d = nullptr, *e = nullptr;
     int *prog = nullptr;
     unsigned *bar = nullptr; // grid-barrier words for cooperative kernels

@@ -1,0 +1,519 @@
+"""cuEV oracle — TEST INFRASTRUCTURE ONLY.
+
+A CPU restatement of the reference solver (ynkrue/cuEV, single-GPU path) used to check the CUDA
+library.  Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU baseline import
+this module, and only as the checker / the timed CPU arm: the product (``cuev_b200``) never
+calls it and has no CPU fallback.
+
+Stages and the reference code each one restates (paths inside the cuEV project):
+
+* ``glibc_fill``          test/cuda/test.h:74-78 ``fill_random`` (srand + rand()%2000 grid), via
+                          the C library's own rand() so the inputs are the reference tests' inputs
+* ``dbbr_panel_qr``       src/cuda/dbbr.cu:124-143 (geqrf -> extract reflectors -> G = Y^T Y ->
+                          larft recurrence dbbr.cu:86-109); LAPACK dgeqrf stands in for cuSOLVER's
+* ``dbbr_reduce``         src/cuda/dbbr.cu:145-229 (double-blocked band reduction, panel order,
+                          deferral correction, green update, per-block SYR2K)
+* ``bc_pack``             src/cuda/dbbr.cu:31-39
+* ``bc_chase``            src/cuda/bulge.cu:64-224 (C code in oracle_kernels.c)
+* ``tridi_dc``            src/cuda/tridi.cu:106-452 (stedx -> laex0 -> laex1 -> laex3), calling
+                          the same LAPACK pieces dsteqr/dlaed2/dlaed4/dlamrg through scipy's
+                          bundled OpenBLAS
+* ``bc_back``/``sbr_back`` src/cuda/backtransform.cu:58-62 and :210-230
+* ``symm_eig_solve``      src/cuda/solver.cu:25-73
+
+Pinning: tests/test_oracle.py checks every stage against the reference's own invariant tests
+(test/cuda/test_*.cu, same inputs and tolerances) and the full solve against LAPACK dsyevd.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import glob
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+BUILD = HERE / "_build"
+LIB = BUILD / "liboracle.so"
+
+SMLSIZ = 64  # src/cuda/tridi.cu:63
+
+
+# ------------------------------------------------------------------------------------------
+# build / load the C part
+# ------------------------------------------------------------------------------------------
+def build() -> Path:
+    BUILD.mkdir(exist_ok=True)
+    src = HERE / "oracle_kernels.c"
+    if not LIB.exists() or LIB.stat().st_mtime < src.stat().st_mtime:
+        subprocess.run(["gcc", "-O2", "-fPIC", "-shared", "-fopenmp", "-o", str(LIB), str(src),
+                        "-lm"], check=True)
+    return LIB
+
+
+_ck = None
+
+
+def _ckern():
+    global _ck
+    if _ck is None:
+        if not LIB.exists():
+            build()
+        L = C.CDLL(str(LIB))
+        dp = C.POINTER(C.c_double)
+        L.oracle_bc_chase.argtypes = [dp, C.c_int, C.c_int, dp, C.c_long, dp, dp]
+        L.oracle_bc_back.argtypes = [dp, C.c_long, dp, C.c_long, C.c_int, C.c_int, C.c_int]
+        _ck = L
+    return _ck
+
+
+def _dp(a: np.ndarray, offset: int = 0):
+    return C.cast(a.ctypes.data + 8 * offset, C.POINTER(C.c_double))
+
+
+def _ip(a: np.ndarray, offset: int = 0):
+    return C.cast(a.ctypes.data + 4 * offset, C.POINTER(C.c_int))
+
+
+# ------------------------------------------------------------------------------------------
+# LAPACK pieces (scipy's OpenBLAS exports them with a scipy_ prefix, LP64)
+# ------------------------------------------------------------------------------------------
+_lp = None
+
+
+def _lapack():
+    global _lp
+    if _lp is None:
+        import scipy
+        libs = glob.glob(os.path.join(os.path.dirname(scipy.__file__), os.pardir, "scipy.libs",
+                                      "libscipy_openblas*.so"))
+        if not libs:
+            raise RuntimeError("scipy's bundled OpenBLAS not found")
+        _lp = C.CDLL(libs[0])
+    return _lp
+
+
+def _ref(v, t=C.c_int):
+    return C.byref(t(v))
+
+
+def lap_steqr(n: int, d: np.ndarray, e: np.ndarray, Z: np.ndarray, ldz: int, zoff: int = 0,
+              doff: int = 0) -> int:
+    """dsteqr('I') on d[doff:doff+n], e[doff:doff+n-1] into Z (Fortran, ld ldz) at zoff."""
+    work = np.zeros(max(1, 2 * n - 2), dtype=np.float64)
+    info = C.c_int(0)
+    _lapack().scipy_dsteqr_(C.c_char_p(b"I"), _ref(n), _dp(d, doff), _dp(e, doff), _dp(Z, zoff),
+                            _ref(ldz), _dp(work), C.byref(info), C.c_size_t(1))
+    return info.value
+
+
+def lap_laed4(k: int, i: int, dl: np.ndarray, w: np.ndarray, delta_out: np.ndarray,
+              doff: int, rho: float) -> tuple[float, int]:
+    dlam = C.c_double(0.0)
+    info = C.c_int(0)
+    _lapack().scipy_dlaed4_(_ref(k), _ref(i), _dp(dl), _dp(w), _dp(delta_out, doff),
+                            _ref(rho, C.c_double), C.byref(dlam), C.byref(info))
+    return dlam.value, info.value
+
+
+# ------------------------------------------------------------------------------------------
+# inputs
+# ------------------------------------------------------------------------------------------
+def glibc_fill(count: int, seed: int, scale: int = 1000) -> np.ndarray:
+    """The reference tests' fill_random (test/cuda/test.h:74-78): srand(seed), then
+    (rand() % (2*scale) - scale) / scale, drawn from the C library's rand()."""
+    libc = C.CDLL("libc.so.6")
+    libc.srand(C.c_uint(seed))
+    r = np.fromiter((libc.rand() for _ in range(count)), dtype=np.int64, count=count)
+    return ((r % (2 * scale)) - scale).astype(np.float64) / scale
+
+
+def sym_from_lower(A0: np.ndarray) -> np.ndarray:
+    L = np.tril(A0)
+    return L + np.tril(A0, -1).T
+
+
+# ------------------------------------------------------------------------------------------
+# Stage 1: DBBR
+# ------------------------------------------------------------------------------------------
+def larft(Y: np.ndarray, tau: np.ndarray) -> np.ndarray:
+    """T from G = Y^T Y and tau, columnwise recurrence T[0:i, i] = -tau_i T[0:i,0:i] G[0:i, i]
+    (src/cuda/dbbr.cu:86-109)."""
+    b = Y.shape[1]
+    G = Y.T @ Y
+    T = np.zeros((b, b))
+    for i in range(b):
+        T[i, i] = tau[i]
+        if i:
+            T[:i, i] = -tau[i] * (T[:i, :i] @ G[:i, i])
+    return T
+
+
+def dbbr_panel_qr(panel: np.ndarray):
+    """Panel QR (src/cuda/dbbr.cu:124-143): returns (packed QR like geqrf, Y, tau, T)."""
+    from scipy.linalg import lapack
+    rows, b = panel.shape
+    qr, tau, _, info = lapack.dgeqrf(np.asfortranarray(panel.copy()))
+    assert info == 0
+    tau_full = np.zeros(b)
+    tau_full[:len(tau)] = tau
+    Y = np.tril(qr, -1)[:, :b]
+    for c in range(min(rows, b)):
+        Y[c, c] = 1.0
+    return qr, Y, tau_full, larft(Y, tau_full)
+
+
+def dbbr_reduce(A0: np.ndarray, b: int, k: int):
+    """Double-blocked band reduction (src/cuda/dbbr.cu:145-229).
+
+    A0: n x n (lower triangle used).  Returns (A, Y, W, Tp) where A's lower band holds the band,
+    Y/W the reflectors (W = Y T per panel) and Tp maps panel start j -> T_j."""
+    A = np.array(A0, dtype=np.float64, order="F", copy=True)
+    n = A.shape[0]
+    Y = np.zeros((n, n), order="F")
+    W = np.zeros((n, n), order="F")
+    Z = np.zeros((n, k), order="F")
+    Tp = {}
+    for i in range(0, n, k):
+        kc = min(k, n - i)
+        w = 0
+        j = i
+        while j < i + kc and j + b < n:
+            pc = b
+            r0 = j + pc
+            qr, Yp, tau, T = dbbr_panel_qr(A[r0:, j:j + pc])
+            A[r0:, j:j + pc] = qr
+            Y[r0:, j:j + pc] = Yp
+            Tp[j] = T
+            Wp = Yp @ T
+            W[r0:, j:j + pc] = Wp
+            At = sym_from_lower(A[r0:, r0:])
+            P = At @ Wp
+            if w > 0:
+                Yb = Y[r0:, i:i + w]
+                Zb = Z[r0:, :w]
+                P -= Yb @ (Zb.T @ Wp) + Zb @ (Yb.T @ Wp)
+            Cm = Wp.T @ P
+            Z[r0:, j - i:j - i + pc] = P - 0.5 * Yp @ Cm
+            w += pc
+            if j + pc < i + kc:
+                Zb = Z[r0:, :w]
+                Yb = Y[r0:, i:i + w]
+                A[r0:, r0:r0 + pc] -= Zb @ Y[r0:r0 + pc, i:i + w].T + Yb @ Z[r0:r0 + pc, :w].T
+            j += b
+        t0 = i + kc
+        if t0 < n and w > 0:
+            Yt = Y[t0:, i:i + w]
+            Zt = Z[t0:, :w]
+            upd = Yt @ Zt.T + Zt @ Yt.T
+            A[t0:, t0:] -= np.tril(upd)
+    return A, Y, W, Tp
+
+
+def bc_pack(A: np.ndarray, b: int) -> np.ndarray:
+    """B[r + j 2b] = A[j+r, j] for r <= b, else 0 (src/cuda/dbbr.cu:31-39).  Fortran (2b, n)."""
+    n = A.shape[0]
+    B = np.zeros((2 * b, n), order="F")
+    for r in range(b + 1):
+        idx = np.arange(n - r)
+        B[r, idx] = A[idx + r, idx]
+    return B
+
+
+def band_dense(B: np.ndarray, b: int, rows: int | None = None) -> np.ndarray:
+    """Dense symmetric matrix from a packed band (first ``rows`` packed rows, default b+1)."""
+    n = B.shape[1]
+    rows = b + 1 if rows is None else rows
+    S = np.zeros((n, n))
+    for r in range(rows):
+        idx = np.arange(n - r)
+        S[idx + r, idx] = B[r, idx]
+        S[idx, idx + r] = B[r, idx]
+    return S
+
+
+# ------------------------------------------------------------------------------------------
+# Stage 2: bulge chasing
+# ------------------------------------------------------------------------------------------
+def bc_chase(B: np.ndarray, b: int):
+    """Sequential bulge chase (src/cuda/bulge.cu:64-224).  Returns (d, e, U, B_out)."""
+    Bw = np.array(B, dtype=np.float64, order="F", copy=True)
+    n = Bw.shape[1]
+    U = np.zeros((n, n), order="F")
+    d = np.zeros(n)
+    e = np.zeros(max(n - 1, 1))
+    _ckern().oracle_bc_chase(_dp(Bw), n, b, _dp(U), n, _dp(d), _dp(e))
+    return d, e[:max(n - 1, 0)], U, Bw
+
+
+def tridiag_dense(d: np.ndarray, e: np.ndarray) -> np.ndarray:
+    return np.diag(d) + np.diag(e, 1) + np.diag(e, -1)
+
+
+# ------------------------------------------------------------------------------------------
+# Stage 3: tridiagonal divide and conquer (reference host D&C, LAPACK pieces)
+# ------------------------------------------------------------------------------------------
+def _laex3(k, n, n1, d, Q, ldq, qoff, rho, dlamda, Q2, indx, ctot, w):
+    """src/cuda/tridi.cu:128-235 (roots, Loewner weights, rank-1 eigenvectors, 2 GEMMs)."""
+    if k == 0:
+        return
+    # roots: column j of Q[0:k, 0:k] receives the delta vector of root j
+    for j in range(k):
+        lam, info = lap_laed4(k, j + 1, dlamda, w, Q, qoff + j * ldq, rho)
+        if info != 0:
+            raise RuntimeError(f"dlaed4 failed, info = {info}")
+        d[j] = lam
+    Qv = lambda i, j: Q[qoff + i + j * ldq]  # noqa: E731
+    if k == 2:
+        for j in range(2):
+            t = [Qv(0, j), Qv(1, j)]
+            Q[qoff + 0 + j * ldq] = t[indx[0] - 1]
+            Q[qoff + 1 + j * ldq] = t[indx[1] - 1]
+    elif k != 1:
+        D = np.array([[Qv(i, j) for j in range(k)] for i in range(k)])  # deltas, D[i, j]
+        s = w[:k].copy()
+        wn = np.empty(k)
+        dl = dlamda[:k]
+        for i in range(k):
+            wi = D[i, i]
+            for j in range(k):
+                if j != i:
+                    wi *= D[i, j] / (dl[i] - dl[j])
+            wn[i] = np.copysign(np.sqrt(-wi), s[i])
+        w[:k] = wn
+        S = wn[:, None] / D
+        S /= np.linalg.norm(S, axis=0)[None, :]
+        perm = np.asarray(indx[:k]) - 1
+        S = S[perm, :]
+        for j in range(k):
+            for i in range(k):
+                Q[qoff + i + j * ldq] = S[i, j]
+    n2 = n - n1
+    n12 = ctot[0] + ctot[1]
+    n23 = ctot[1] + ctot[2]
+    iq2 = n1 * n12
+    Sm = np.array([[Q[qoff + i + j * ldq] for j in range(k)] for i in range(k)])
+    out2 = None
+    if n23 != 0:
+        Q2b = Q2[iq2:iq2 + n2 * n23].reshape((n2, n23), order="F")
+        out2 = Q2b @ Sm[ctot[0]:ctot[0] + n23, :]
+    out1 = None
+    if n12 != 0:
+        Q2a = Q2[:n1 * n12].reshape((n1, n12), order="F")
+        out1 = Q2a @ Sm[:n12, :]
+    for j in range(k):
+        col = qoff + j * ldq
+        Q[col + n1:col + n] = out2[:, j] if out2 is not None else 0.0
+        Q[col:col + n1] = out1[:, j] if out1 is not None else 0.0
+
+
+def _laex1(n, d, doff, Q, ldq, qoff, indxq, ioff, rho, cutpnt, work):
+    """src/cuda/tridi.cu:241-263: z from the split eigenvectors, dlaed2 deflation, laex3."""
+    z = np.empty(n)
+    for i in range(cutpnt):
+        z[i] = Q[qoff + (cutpnt - 1) + i * ldq]
+    for i in range(cutpnt, n):
+        z[i] = Q[qoff + cutpnt + i * ldq]
+    dlamda = np.zeros(n)
+    w = np.zeros(n)
+    Q2 = np.zeros(n * n)
+    indx = np.zeros(n, dtype=np.int32)
+    indxc = np.zeros(n, dtype=np.int32)
+    indxp = np.zeros(n, dtype=np.int32)
+    coltyp = np.zeros(n, dtype=np.int32)
+    kk = C.c_int(0)
+    info = C.c_int(0)
+    rho_c = C.c_double(rho)
+    dl = d  # view with offset
+    _lapack().scipy_dlaed2_(C.byref(kk), _ref(n), _ref(cutpnt), _dp(dl, doff), _dp(Q, qoff),
+                            _ref(ldq), _ip(indxq, ioff), C.byref(rho_c), _dp(z), _dp(dlamda),
+                            _dp(w), _dp(Q2), _ip(indx), _ip(indxc), _ip(indxp), _ip(coltyp),
+                            C.byref(info))
+    if info.value != 0:
+        raise RuntimeError(f"dlaed2 failed, info = {info.value}")
+    k = kk.value
+    if k != 0:
+        dsub = d[doff:doff + n]  # numpy view (shares memory)
+        _laex3(k, n, cutpnt, dsub, Q, ldq, qoff, rho_c.value, dlamda, Q2, indxc, coltyp[:4],
+               w)
+        idx = np.zeros(n, dtype=np.int32)
+        _lapack().scipy_dlamrg_(_ref(k), _ref(n - k), _dp(d, doff), _ref(1), _ref(-1), _ip(idx))
+        indxq[ioff:ioff + n] = idx
+    else:
+        indxq[ioff:ioff + n] = np.arange(1, n + 1)
+
+
+def _laex0(n, d, e, off, Q, ldq, indxq):
+    """src/cuda/tridi.cu:268-339 on the block starting at global index ``off``."""
+    part = [n]
+    while part[-1] > SMLSIZ:
+        new = []
+        for p in part:
+            new += [p // 2, (p + 1) // 2]
+        part = new
+    # the reference fills part[2j-2] = p//2, part[2j-1] = (p+1)//2 from the end
+    cum = np.cumsum(part).tolist()
+    subpbs = len(part)
+    for i in range(subpbs - 1):
+        sm = cum[i]
+        d[off + sm - 1] -= abs(e[off + sm - 1])
+        d[off + sm] -= abs(e[off + sm - 1])
+    for i in range(subpbs):
+        sm = 0 if i == 0 else cum[i - 1]
+        ms = cum[0] if i == 0 else cum[i] - cum[i - 1]
+        info = lap_steqr(ms, d, e, Q, ldq, zoff=(off + sm) + (off + sm) * ldq, doff=off + sm)
+        if info != 0:
+            raise RuntimeError(f"dsteqr (leaf) failed, info = {info}")
+        indxq[off + sm:off + sm + ms] = np.arange(1, ms + 1)
+    work = None
+    while subpbs > 1:
+        for i in range(0, subpbs - 1, 2):
+            if i == 0:
+                sm, ms, msd2 = 0, cum[1], cum[0]
+            else:
+                sm = cum[i - 1]
+                ms = cum[i + 1] - cum[i - 1]
+                msd2 = ms // 2
+            _laex1(ms, d, off + sm, Q, ldq, (off + sm) + (off + sm) * ldq, indxq, off + sm,
+                   e[off + sm + msd2 - 1], msd2, work)
+            cum[i // 2] = cum[i + 1]
+        subpbs //= 2
+    # reorder columns by indxq (ascending eigenvalues)
+    perm = indxq[off:off + n] - 1
+    dd = d[off:off + n][perm].copy()
+    blk = np.empty((n, n))
+    for i in range(n):
+        c = off + perm[i]
+        blk[:, i] = Q[(off + c * ldq):(off + c * ldq + n)]
+    d[off:off + n] = dd
+    for i in range(n):
+        Q[(off + (off + i) * ldq):(off + (off + i) * ldq + n)] = blk[:, i]
+
+
+def tridi_dc(d_in: np.ndarray, e_in: np.ndarray):
+    """Eigen-decomposition of tridiag(d, e) following src/cuda/tridi.cu:345-452 (stedx).
+    Returns (eval ascending, evec n x n)."""
+    n = len(d_in)
+    d = np.array(d_in, dtype=np.float64).copy()
+    e = np.zeros(n)
+    e[:n - 1] = e_in[:n - 1]
+    Qf = np.zeros(n * n)
+    Qf[::n + 1] = 1.0
+    if n < SMLSIZ:
+        info = lap_steqr(n, d, e, Qf, n)
+        if info != 0:
+            raise RuntimeError(f"dsteqr failed, info = {info}")
+        return d, Qf.reshape((n, n), order="F").copy()
+    orgnrm = max(np.abs(d).max(), np.abs(e[:n - 1]).max() if n > 1 else 0.0)
+    if orgnrm == 0:
+        return d, Qf.reshape((n, n), order="F").copy()
+    eps = np.finfo(np.float64).eps
+    indxq = np.zeros(n, dtype=np.int32)
+    start = 0
+    last_m = n
+    while start < n:
+        end = start + 1
+        while end < n:
+            tiny = eps * np.sqrt(abs(d[end - 1] * d[end]))
+            if abs(e[end - 1]) <= tiny:
+                break
+            end += 1
+        m = end - start
+        last_m = m
+        if m == 1:
+            start = end
+            continue
+        if m > SMLSIZ:
+            bn = max(np.abs(d[start:end]).max(), np.abs(e[start:end - 1]).max())
+            d[start:end] /= bn
+            e[start:end - 1] /= bn
+            _laex0(m, d, e, start, Qf, n, indxq)
+            d[start:end] *= bn
+        else:
+            info = lap_steqr(m, d, e, Qf, n, zoff=start + start * n, doff=start)
+            if info != 0:
+                raise RuntimeError(f"dsteqr (block) failed, info = {info}")
+        start = end
+    Q = Qf.reshape((n, n), order="F").copy()
+    if last_m < n:
+        order = np.argsort(d, kind="stable")
+        d = d[order]
+        Q = Q[:, order]
+    return d, Q
+
+
+# ------------------------------------------------------------------------------------------
+# Stage 4: back-transform
+# ------------------------------------------------------------------------------------------
+def bc_back(U: np.ndarray, M: np.ndarray, b: int) -> np.ndarray:
+    """M <- Q_b M (src/cuda/backtransform.cu:58-62); C code, columns in parallel."""
+    n = U.shape[0]
+    Mo = np.array(M, dtype=np.float64, order="F", copy=True)
+    Uf = np.asfortranarray(U)
+    _ckern().oracle_bc_back(_dp(Uf), n, _dp(Mo), Mo.shape[0], n, Mo.shape[1], b)
+    return Mo
+
+
+def sbr_back(Y: np.ndarray, W: np.ndarray, M: np.ndarray, b: int) -> np.ndarray:
+    """M <- Q_s M: panels from last to first, Mb -= W (Y^T Mb) (backtransform.cu:210-230)."""
+    n = Y.shape[0]
+    Mo = np.array(M, dtype=np.float64, order="F", copy=True)
+    jmax = 0
+    j = 0
+    while j + b < n:
+        jmax = j
+        j += b
+    for j in range(jmax, -1, -b):
+        if j + b >= n:
+            continue
+        r0 = j + b
+        Yp = Y[r0:, j:j + b]
+        Wp = W[r0:, j:j + b]
+        Mo[r0:, :] -= Wp @ (Yp.T @ Mo[r0:, :])
+    return Mo
+
+
+# ------------------------------------------------------------------------------------------
+# Full solve
+# ------------------------------------------------------------------------------------------
+def symm_eig_solve(A0: np.ndarray, b: int = 32, k: int = 512, timings: dict | None = None):
+    """The reference pipeline (src/cuda/solver.cu:25-73) on the CPU: returns (eval, evec)."""
+    import time
+    n = A0.shape[0]
+    if n == 0:
+        return np.zeros(0), np.zeros((0, 0))
+    if n == 1:
+        return np.array([A0[0, 0]]), np.ones((1, 1))
+    t0 = time.perf_counter()
+    A, Y, W, _ = dbbr_reduce(A0, b, k)
+    B = bc_pack(A, b)
+    t1 = time.perf_counter()
+    d, e, U, _ = bc_chase(B, b)
+    t2 = time.perf_counter()
+    w, Qd = tridi_dc(d, e)
+    t3 = time.perf_counter()
+    V = sbr_back(Y, W, bc_back(U, Qd, b), b)
+    t4 = time.perf_counter()
+    if timings is not None:
+        timings.update(dbbr_s=t1 - t0, bc_s=t2 - t1, dc_s=t3 - t2, bt_s=t4 - t3)
+    return w, V
+
+
+# ------------------------------------------------------------------------------------------
+# Metrics (both normalisations used by the reference and the build)
+# ------------------------------------------------------------------------------------------
+def metrics(A: np.ndarray, w: np.ndarray, V: np.ndarray, w_ref: np.ndarray | None = None):
+    n = A.shape[0]
+    R = A @ V - V * w[None, :]
+    anorm_f = np.linalg.norm(A)
+    anorm_2 = np.abs(w_ref if w_ref is not None else w).max() if n else 1.0
+    out = {
+        "resid_fro_rel": float(np.linalg.norm(R) / max(anorm_f, 1e-300)),   # bench_solver.cpp:117
+        "resid_n_norm2": float(np.linalg.norm(R) / max(n * anorm_2, 1e-300)),
+        "orth_fro": float(np.linalg.norm(V.T @ V - np.eye(n))),
+    }
+    if w_ref is not None:
+        out["max_dlambda_rel"] = float(np.abs(w - w_ref).max() / max(anorm_2, 1e-300))
+    return out
