@@ -216,8 +216,10 @@ template <int BW> int launch_panel_qr(Workspace *ws, double *A, long long lda, d
     const int sms = num_sms();
     int P = std::max(1, std::min(sms, div_up(rows, QR_TARGET_ROWS)));
     int chunk = div_up(rows, P);
+    auto kern = panel_qr_kernel<BW>;
     // shared memory bound: grow P (up to one CTA per SM) if the chunk does not fit
-    const size_t max_smem = 227 * 1024;
+    static size_t max_smem = 0;
+    if (max_smem == 0) max_smem = max_dynamic_smem((const void *)kern);
     while (panel_qr_smem<BW>(chunk) > max_smem && P < sms) {
         ++P;
         chunk = div_up(rows, P);
@@ -231,7 +233,6 @@ template <int BW> int launch_panel_qr(Workspace *ws, double *A, long long lda, d
         return CUEV_ERR_INVALID;
     }
     const size_t smem = panel_qr_smem<BW>(chunk);
-    auto kern = panel_qr_kernel<BW>;
     static bool attr = false;
     if (!attr) {
         CUEV_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,

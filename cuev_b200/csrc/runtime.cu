@@ -32,6 +32,16 @@ int num_sms() {
     return cached[dev];
 }
 
+size_t max_dynamic_smem(const void *func) {
+    int dev = 0, optin = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+        optin = 227 * 1024;
+    cudaFuncAttributes fa{};
+    if (cudaFuncGetAttributes(&fa, func) != cudaSuccess) return 0;
+    return (size_t)optin > fa.sharedSizeBytes ? (size_t)optin - fa.sharedSizeBytes : 0;
+}
+
 } // namespace cuev
 
 extern "C" const char *cuev_last_error(void) { return cuev::g_last_error.c_str(); }

@@ -36,7 +36,7 @@ struct Workspace {
     size_t splitk_bytes = 0;
 
     // D&C
-    double *dc_Q2 = nullptr, *dc_S = nullptr, *dc_vec = nullptr;
+    double *dc_Q2 = nullptr, *dc_S = nullptr, *dc_T = nullptr, *dc_vec = nullptr;
     int *dc_int = nullptr;
     size_t dc_vec_elems = 0, dc_int_elems = 0;
     GemmArgs *dc_gemm_args = nullptr;

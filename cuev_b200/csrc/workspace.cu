@@ -40,6 +40,7 @@ int workspace_create(int n, int b, int k, cudaStream_t stream, Workspace **out) 
         {(void **)&ws->U, nn * s},
         {(void **)&ws->dc_Q2, nn * s},
         {(void **)&ws->dc_S, nn * s},
+        {(void **)&ws->dc_T, nn * s},
         {(void **)&ws->Z, N * k * s},
         {(void **)&ws->Wp, N * b * s},
         {(void **)&ws->Tp, (N / b + 2) * b * b * s},
