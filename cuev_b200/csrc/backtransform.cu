@@ -118,7 +118,7 @@ template <int BW, int TS> int launch_bc_back(Workspace *ws, double *M, long long
     constexpr int NWARP = 2;
     const int grid = div_up(ncols, 32 * NWARP);
     bc_back_kernel<BW, TS, NWARP><<<grid, 32 * NWARP, 0, ws->stream>>>(ws->U, ws->n, M, ldm,
-                                                                       ws->n, ncols);
+                                                                       ws->n, ncols); note_launch();
     CUEV_TRY(cudaGetLastError());
     return CUEV_OK;
 }

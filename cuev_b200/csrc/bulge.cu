@@ -222,6 +222,7 @@ template <int BW> int launch_chase(Workspace *ws, double *B) {
     long long ldu = n;
     int nn = n, bb = b;
     void *args[] = {&B, &U, &ldu, &nn, &bb, &ws->prog, &ws->status};
+    note_launch();
     CUEV_TRY(cudaLaunchCooperativeKernel((void *)kern, dim3(grid), dim3(BC_THREADS), args, smem,
                                          ws->stream));
     return CUEV_OK;
@@ -244,7 +245,7 @@ int bc_chase(Workspace *ws, double *B, double *d, double *e) {
     }
     if (n > 0) {
         bc_extract_kernel<<<std::max(1, std::min(1024, div_up(n, 256))), 256, 0, ws->stream>>>(
-            B, d, e, n, b);
+            B, d, e, n, b); note_launch();
         CUEV_TRY(cudaGetLastError());
     }
     return CUEV_OK;

@@ -105,7 +105,7 @@ int solve_d(double *A, int n, double *eval, double *evec, cudaStream_t stream, c
     if (!A || !eval || !evec) return CUEV_ERR_INVALID;
     auto wall0 = std::chrono::high_resolution_clock::now();
     if (n == 1) {
-        small_solve_kernel<<<1, 1, 0, stream>>>(A, eval, evec);
+        small_solve_kernel<<<1, 1, 0, stream>>>(A, eval, evec); note_launch();
         CUEV_TRY(cudaGetLastError());
         CUEV_TRY(cudaStreamSynchronize(stream));
         if (timer) *timer = cuev_timer{};
@@ -128,7 +128,7 @@ int solve_d(double *A, int n, double *eval, double *evec, cudaStream_t stream, c
         if (timer) CUEV_TRY(cudaEventRecord(ev.e[i], stream));
         return CUEV_OK;
     };
-    nonfinite_scan_kernel<<<4 * num_sms(), 256, 0, stream>>>(A, n, n, ws->status);
+    nonfinite_scan_kernel<<<4 * num_sms(), 256, 0, stream>>>(A, n, n, ws->status); note_launch();
     CUEV_TRY(cudaGetLastError());
     CUEV_CHECK_STATUS(workspace_check_status(ws, "input scan"));
 
@@ -201,12 +201,12 @@ extern "C" int cuev_ssyevd(float *A, int n, float *eval, float *evec, void *stre
     }
     double *A64 = buf, *V64 = buf + nn, *w64 = buf + 2 * nn;
     const int blocks = 4 * num_sms();
-    widen_kernel<<<blocks, 256, 0, st>>>(A, A64, nn);
+    widen_kernel<<<blocks, 256, 0, st>>>(A, A64, nn); note_launch();
     int s = solve_d(A64, n, w64, V64, st, timer, nullptr);
     if (s == CUEV_OK) {
-        narrow_kernel<<<blocks, 256, 0, st>>>(V64, evec, nn);
-        narrow_kernel<<<1, 256, 0, st>>>(w64, eval, n);
-        narrow_kernel<<<blocks, 256, 0, st>>>(A64, A, nn); // A is clobbered like the reference's
+        narrow_kernel<<<blocks, 256, 0, st>>>(V64, evec, nn); note_launch();
+        narrow_kernel<<<1, 256, 0, st>>>(w64, eval, n); note_launch();
+        narrow_kernel<<<blocks, 256, 0, st>>>(A64, A, nn); note_launch(); // A is clobbered like the reference's
     }
     cudaFreeAsync(buf, st);
     if (cudaStreamSynchronize(st) != cudaSuccess && s == CUEV_OK) s = CUEV_ERR_CUDA;

@@ -37,6 +37,8 @@ inline int div_up(int a, int b) { return (a + b - 1) / b; }
 inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
 int num_sms();
+// Count of kernels this library has launched (exported as cuev_kernel_launches).
+void note_launch(int count = 1);
 // Largest dynamic shared-memory size a kernel may request (opt-in limit minus its static part).
 size_t max_dynamic_smem(const void *func);
 

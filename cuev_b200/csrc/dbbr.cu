@@ -242,6 +242,7 @@ template <int BW> int launch_panel_qr(Workspace *ws, double *A, long long lda, d
     CUEV_TRY(cudaMemsetAsync(ws->bar, 0, 2 * sizeof(unsigned), ws->stream));
     void *args[] = {&A, &lda, &Y, &ldy, &tau, &T, &W, &ldw, &rows, &b, &chunk,
                     &ws->qr_part, &ws->bar, &ws->status};
+    note_launch();
     CUEV_TRY(cudaLaunchCooperativeKernel((void *)kern, dim3(P), dim3(QR_THREADS), args, smem,
                                          ws->stream));
     return CUEV_OK;
@@ -261,7 +262,7 @@ int panel_qr(Workspace *ws, double *A, long long lda, double *Y, long long ldy, 
 int dbbr_pack(Workspace *ws, const double *A, long long lda, double *B) {
     const long long total = 2LL * ws->b * ws->n;
     const int blocks = (int)std::min<long long>(8LL * num_sms(), (total + 255) / 256);
-    pack_kernel<<<std::max(1, blocks), 256, 0, ws->stream>>>(A, lda, B, ws->n, ws->b);
+    pack_kernel<<<std::max(1, blocks), 256, 0, ws->stream>>>(A, lda, B, ws->n, ws->b); note_launch();
     CUEV_TRY(cudaGetLastError());
     return CUEV_OK;
 }

@@ -253,7 +253,7 @@ int launch_cfg(const GemmArgs &a, const GemmArgs *dev_args, dim3 grid, cudaStrea
                                       (int)L::BYTES));
         attr_set = true;
     }
-    kern<<<grid, C::NT, L::BYTES, stream>>>(a, dev_args);
+    kern<<<grid, C::NT, L::BYTES, stream>>>(a, dev_args); note_launch();
     CUEV_TRY(cudaGetLastError());
     return CUEV_OK;
 }
@@ -313,7 +313,7 @@ int gemm_launch(const GemmArgs &a_in, int ta, int tb, cudaStream_t stream) {
     if (ktot <= 0 || a.alpha == 0.0) {
         // C = beta C on the (masked) output; reuse the reduction kernel with zero splits.
         splitk_reduce_kernel<<<std::min(4096, div_up(a.m * a.n, 256)), 256, 0, stream>>>(
-            a.m, a.n, 0, nullptr, a.beta, a.C, a.ldc, a.c_lower);
+            a.m, a.n, 0, nullptr, a.beta, a.C, a.ldc, a.c_lower); note_launch();
         CUEV_TRY(cudaGetLastError());
         return CUEV_OK;
     }
@@ -343,7 +343,7 @@ int gemm_launch(const GemmArgs &a_in, int ta, int tb, cudaStream_t stream) {
         const long long total = (long long)a.m * a.n;
         const int blocks = (int)std::min<long long>(4 * num_sms(), (total + 255) / 256);
         splitk_reduce_kernel<<<blocks, 256, 0, stream>>>(a.m, a.n, a.splits, a.ws, a.beta, a.C,
-                                                         a.ldc, a.c_lower);
+                                                         a.ldc, a.c_lower); note_launch();
         CUEV_TRY(cudaGetLastError());
     }
     return CUEV_OK;

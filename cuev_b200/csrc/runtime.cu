@@ -1,6 +1,7 @@
 // Host runtime pieces shared by all stages: last-error bookkeeping, device properties.
 #include "common.cuh"
 
+#include <atomic>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -9,7 +10,10 @@ namespace cuev {
 
 namespace {
 thread_local std::string g_last_error;
-}
+std::atomic<long long> g_launches{0};
+} // namespace
+
+void note_launch(int count) { g_launches.fetch_add(count, std::memory_order_relaxed); }
 
 void set_last_error(cudaError_t e, const char *file, int line) {
     char buf[512];
@@ -45,3 +49,5 @@ size_t max_dynamic_smem(const void *func) {
 } // namespace cuev
 
 extern "C" const char *cuev_last_error(void) { return cuev::g_last_error.c_str(); }
+
+extern "C" long long cuev_kernel_launches(void) { return cuev::g_launches.load(); }

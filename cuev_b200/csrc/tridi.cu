@@ -750,12 +750,12 @@ int tridi_dc(Workspace *ws, const double *d, const double *e, double *eval, doub
     CUEV_TRY(cudaMemcpyAsync(dbase, hbuf.data(), hbuf.size(), cudaMemcpyHostToDevice, st));
 
     // scale, clear Q, leaves
-    dc_norm_kernel<<<1, 1024, 0, st>>>(d, e, n, a.scale, ws->status);
+    dc_norm_kernel<<<1, 1024, 0, st>>>(d, e, n, a.scale, ws->status); note_launch();
     dc_scale_in_kernel<<<std::max(1, std::min(1024, div_up(n, 256))), 256, 0, st>>>(d, e, eval,
-                                                                                   a.E, n, a.scale);
+                                                                                   a.E, n, a.scale); note_launch();
     CUEV_TRY(cudaMemsetAsync(evec, 0, sizeof(double) * (size_t)n * n, st));
     dc_leaf_kernel<<<(int)leaves.size(), 32, 0, st>>>(d_leaves, eval, a.E, evec, ldq, n,
-                                                      ws->status);
+                                                      ws->status); note_launch();
     CUEV_TRY(cudaGetLastError());
 
     double *Q2 = ws->dc_Q2, *Dl = ws->dc_S, *S = ws->dc_T;
@@ -763,24 +763,24 @@ int tridi_dc(Workspace *ws, const double *d, const double *e, double *eval, doub
         const int cnt = lvl_count[li];
         const MergeDesc *dd = d_descs + lvl_start[li];
         const int maxnm = lvl_maxnm[li];
-        dc_deflate_kernel<<<cnt, DF_THREADS, 0, st>>>(dd, eval, evec, ldq, a);
-        dc_rotate_kernel<<<dim3(div_up(maxnm, 128), cnt), 128, 0, st>>>(dd, evec, ldq, Q2, a);
-        dc_secular_kernel<<<div_up(n * 32, 256), 256, 0, st>>>(dd, cnt, n, Dl, a, ws->status);
-        dc_lowner_kernel<<<div_up(n, 256), 256, 0, st>>>(dd, cnt, n, Dl, a);
-        dc_svec_kernel<<<div_up(n * 32, 256), 256, 0, st>>>(dd, cnt, n, Dl, S, a);
+        dc_deflate_kernel<<<cnt, DF_THREADS, 0, st>>>(dd, eval, evec, ldq, a); note_launch();
+        dc_rotate_kernel<<<dim3(div_up(maxnm, 128), cnt), 128, 0, st>>>(dd, evec, ldq, Q2, a); note_launch();
+        dc_secular_kernel<<<div_up(n * 32, 256), 256, 0, st>>>(dd, cnt, n, Dl, a, ws->status); note_launch();
+        dc_lowner_kernel<<<div_up(n, 256), 256, 0, st>>>(dd, cnt, n, Dl, a); note_launch();
+        dc_svec_kernel<<<div_up(n * 32, 256), 256, 0, st>>>(dd, cnt, n, Dl, S, a); note_launch();
         // Delta is dead now: the GEMM output goes to its region
         dc_gemm_prep_kernel<<<div_up(cnt, 128), 128, 0, st>>>(dd, cnt, Q2, S, Dl, ws->dc_gemm_args,
-                                                              a);
+                                                              a); note_launch();
         CUEV_TRY(cudaGetLastError());
         CUEV_CHECK_STATUS(gemm_batched_launch(ws->dc_gemm_args, 2 * cnt, lvl_maxm[li], maxnm, 0, 0,
                                               st));
-        dc_order_kernel<<<cnt, 512, 0, st>>>(dd, eval, a);
+        dc_order_kernel<<<cnt, 512, 0, st>>>(dd, eval, a); note_launch();
         dc_permute_kernel<<<dim3(div_up(maxnm, 128), maxnm, cnt), 128, 0, st>>>(dd, evec, ldq, Dl,
-                                                                               Q2, a);
+                                                                               Q2, a); note_launch();
         CUEV_TRY(cudaGetLastError());
     }
     dc_scale_out_kernel<<<std::max(1, std::min(1024, div_up(n, 256))), 256, 0, st>>>(eval, n,
-                                                                                    a.scale);
+                                                                                    a.scale); note_launch();
     CUEV_TRY(cudaGetLastError());
     return CUEV_OK;
 }

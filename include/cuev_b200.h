@@ -79,6 +79,9 @@ int cuev_release_workspace(void);
 /* Message for the last failing call on this host thread ("" if none). */
 const char *cuev_last_error(void);
 
+/* Number of CUDA kernels this library has launched since it was loaded (profiling aid). */
+long long cuev_kernel_launches(void);
+
 /* ---------------------------------------------------------------------------------------------
  * Stage-level API used by the stage tests.  Mirrors the reference's SolverHandle<T> and
  * cuev::kernels::* launchers (include/cuda/handle.h:61-100, include/cuda/kernels.cuh:47-155).
