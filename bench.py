@@ -1,0 +1,395 @@
+#!/usr/bin/env python
+"""Benchmark: dense symmetric eigensolve (all eigenvalues + eigenvectors) on B200.
+
+One "step" is one full solve of an n x n FP64 matrix A = (G + G^T)/2, G iid N(0, 1) from a seed,
+through cuev_b200 (DBBR -> pack -> bulge chase -> GPU D&C -> back-transform).  The headline
+workload is n = 16384, the size the reference's north-star metric is quoted on; the matrix
+(2.1 GB) is far larger than the 126 MB L2, so no flush is needed between steps.
+
+Reported (one JSON line on rank 0):
+  value      whole-job TFLOP/s = world x steps x 6.67 n^3 / (max over ranks of device time)
+             (work model: DBBR 4/3 n^3 + D&C <= 4/3 n^3 + back-transform 4 n^3)
+  e2e        the same metric through the C ABI with HOST buffers: every step copies A from
+             pinned host memory, solves, and copies eval + evec back
+  roofline   the bulge-chasing back-transform kernel (one launch, 2 n^3 FLOP) against the FP64
+             peak measured in the same run (cuBLAS DGEMM 8192^3)
+  cpu_baseline  the oracle (CPU restatement of the reference pipeline) on a bounded sample
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cuev|reference] [--n N]
+Multi-GPU (replicas only: every rank solves its own matrix; no collective on the data path):
+  python -m torch.distributed.run --nproc-per-node N --master-addr 127.0.0.1 bench.py --gpus N
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+FLOP_MODEL = 20.0 / 3.0  # (4/3 + 4/3 + 4) n^3 per solve
+
+
+def _env_int(name, default):
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+def metric_name(n):
+    return f"eigh n={n} FP64 (all eigenpairs), TFLOP/s at 6.67 n^3 per solve"
+
+
+# ------------------------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ------------------------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu_index = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            out = ROOT / "gpurun_out"
+            out.mkdir(exist_ok=True)
+            self.path = out / f"clocks_gpu{self.gpu_index}.csv"
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-i", str(self.gpu_index), "-lms", "200"], stdout=self.fh,
+                stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        loaded = [s for s in sm if s > 0.5 * max(sm)] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------------------------------
+# CPU baseline: the oracle (CPU restatement of the reference pipeline)
+# ------------------------------------------------------------------------------------------
+def cpu_oracle_sample(n_cpu: int, repeats: int = 1):
+    import numpy as np
+    from oracle import cuev_oracle as O  # checker / CPU arm only
+    O.build()
+    rng = np.random.default_rng(4321)
+    G = rng.standard_normal((n_cpu, n_cpu))
+    A = np.asfortranarray((G + G.T) / 2)
+    times = []
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        O.symm_eig_solve(A, 32, 256)
+        times.append(time.perf_counter() - t0)
+    t = statistics.median(times)
+    return FLOP_MODEL * n_cpu ** 3 / t / 1e12, t
+
+
+def lapack_dsyevd_sample(n_cpu: int):
+    import numpy as np
+    import scipy.linalg as sla
+    rng = np.random.default_rng(4321)
+    G = rng.standard_normal((n_cpu, n_cpu))
+    A = (G + G.T) / 2
+    t0 = time.perf_counter()
+    sla.eigh(A, driver="evd")
+    t = time.perf_counter() - t0
+    return FLOP_MODEL * n_cpu ** 3 / t / 1e12, t
+
+
+def run_reference(args, rank, world):
+    """The reference arm: the reference pipeline restated on the host cores (the oracle port;
+    the reference itself has no CPU implementation of the path), on a bounded sample."""
+    if rank != 0:
+        return 0
+    n_cpu = args.cpu_n
+    cores = os.cpu_count()
+    for _ in range(args.warmup):
+        cpu_oracle_sample(n_cpu)
+    vals, secs = [], []
+    for _ in range(args.steps):
+        v, t = cpu_oracle_sample(n_cpu)
+        vals.append(v)
+        secs.append(t)
+    value = statistics.median(vals)
+    line = {
+        "impl": "reference", "metric": metric_name(args.n), "value": round(value, 6),
+        "unit": "TFLOP/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(1000 * statistics.median(secs), 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"eigh A=(G+G^T)/2, G iid N(0,1); bounded CPU sample n={n_cpu}",
+                   "n": args.n, "sample_n": n_cpu},
+        "cpu_baseline": {"value": round(value, 6), "unit": "TFLOP/s", "cores": cores,
+                         "kind": "port",
+                         "sample": f"one full oracle solve at n={n_cpu} per step (median of "
+                                   f"{args.steps}); BLAS calls use all {cores} host threads, "
+                                   "bulge chase and LAPACK D&C pieces run sequentially"},
+        "e2e": {"value": round(value, 6), "unit": "TFLOP/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------------------------------
+# the GPU arm
+# ------------------------------------------------------------------------------------------
+def run_cuev(args, rank, world, local_rank):
+    import ctypes as C
+
+    import torch
+    import cuev_b200 as cv
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=dev)
+    n = args.n
+    lib = cv.lib()
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+
+    # input: A = (G + G^T)/2 (symmetric, so column-major storage == row-major storage)
+    g = torch.Generator(device=dev).manual_seed(1234 + rank)
+    A0 = torch.randn(n, n, dtype=torch.float64, device=dev, generator=g)
+    A0 = (A0 + A0.t()) * 0.5
+    A0 = A0.contiguous()
+    A = torch.empty_like(A0)
+    w = torch.empty(n, dtype=torch.float64, device=dev)
+    V = torch.empty_like(A0)
+    cfg = cv.Config(args.nbw, args.nk)
+    timer = cv.Timer()
+
+    def solve():
+        st = lib.cuev_dsyevd_cfg(A.data_ptr(), n, w.data_ptr(), V.data_ptr(), sp, C.byref(timer),
+                                 C.byref(cfg))
+        if st != 0:
+            raise RuntimeError(f"cuev_dsyevd failed: {st} {lib.cuev_last_error().decode()}")
+
+    for _ in range(max(3, args.warmup)):
+        A.copy_(A0)
+        solve()
+    torch.cuda.synchronize()
+
+    # FP64 peak reference measured in this run: cuBLAS DGEMM 8192^3
+    a = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
+    torch.matmul(a, a)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    best = 1e30
+    for _ in range(3):
+        e0.record()
+        torch.matmul(a, a)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    fp64_peak = 2 * 8192 ** 3 / (best * 1e-3) / 1e12
+    del a
+    torch.cuda.empty_cache()
+
+    # ---- timed region
+    gpu_index = local_rank
+    cvd = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if cvd:
+        ids = [x for x in cvd.split(",") if x.strip()]
+        if local_rank < len(ids) and ids[local_rank].strip().isdigit():
+            gpu_index = int(ids[local_rank])
+    clocks = ClockSampler(gpu_index)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    launches0 = lib.cuev_kernel_launches()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    stage = {"dbbr_ms": [], "bc_ms": [], "dc_ms": [], "bt_qb_ms": [], "bt_qs_ms": []}
+    for i in range(args.steps):
+        A.copy_(A0)  # restore the (overwritten) input outside the timed pair
+        ev[i][0].record(stream)
+        solve()
+        ev[i][1].record(stream)
+        for k2 in stage:
+            stage[k2].append(getattr(timer, k2))
+    torch.cuda.synchronize()
+    launches = lib.cuev_kernel_launches() - launches0
+    clk = clocks.stop()
+    total_ms = sum(e0_.elapsed_time(e1_) for e0_, e1_ in ev)
+    t_max = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+    if dist:
+        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
+    total_ms = float(t_max.item())
+    ms_per = total_ms / args.steps
+    value = world * args.steps * FLOP_MODEL * n ** 3 / (total_ms * 1e-3) / 1e12
+
+    # accuracy of the last solve (device, cuBLAS): ||AV - VL||_F / (n ||A||_2), ||V^T V - I||_F
+    with torch.no_grad():
+        Vl = V.t()  # column-major storage -> logical matrix
+        R = A0 @ Vl - Vl * w[None, :]
+        anorm = w.abs().max()
+        resid = float(torch.linalg.norm(R) / (n * anorm))
+        resid_ref = float(torch.linalg.norm(R) / torch.linalg.norm(A0))
+        del R
+        O_ = Vl.t() @ Vl
+        O_.diagonal().sub_(1.0)
+        orth = float(torch.linalg.norm(O_))
+        del O_
+        torch.cuda.empty_cache()
+
+    # ---- end to end through the C ABI with host buffers
+    e2e = None
+    if not args.no_e2e:
+        hA = torch.empty(n * n, dtype=torch.float64, pin_memory=True)
+        hA.copy_(A0.reshape(-1).cpu())
+        hw = torch.empty(n, dtype=torch.float64, pin_memory=True)
+        hV = torch.empty(n * n, dtype=torch.float64, pin_memory=True)
+        Af = A.reshape(-1)
+        Vf = V.reshape(-1)
+        steps_e2e = max(1, min(args.steps, 2))
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        tot = 0.0
+        for _ in range(steps_e2e):
+            x0, x1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            x0.record(stream)
+            Af.copy_(hA, non_blocking=True)
+            solve()
+            hw.copy_(w, non_blocking=True)
+            hV.copy_(Vf, non_blocking=True)
+            x1.record(stream)
+            torch.cuda.synchronize()
+            tot += x0.elapsed_time(x1)
+        te = torch.tensor([tot], dtype=torch.float64, device=dev)
+        if dist:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        tot = float(te.item())
+        e2e = {"value": round(world * steps_e2e * FLOP_MODEL * n ** 3 / (tot * 1e-3) / 1e12, 4),
+               "unit": "TFLOP/s", "h2d_bytes_per_step": 8 * n * n,
+               "d2h_bytes_per_step": 8 * n * n + 8 * n,
+               "ms_per_step": round(tot / steps_e2e, 3)}
+
+    med = {k2: statistics.median(v) for k2, v in stage.items()}
+    bcb_ms = med["bt_qb_ms"]
+    bcb_flops = 2.0 * n ** 3
+    achieved = bcb_flops / (bcb_ms * 1e-3) / 1e12
+    traffic = None
+    tfile = ROOT / "profiles" / "bc_back_traffic.json"
+    if tfile.exists():
+        try:
+            tj = json.loads(tfile.read_text())
+            # DRAM bytes per launch scale with n^2 (M is read and written once per sweep tile)
+            traffic = int(tj["dram_bytes"] * (n / tj["n"]) ** 3)
+        except Exception:
+            traffic = None
+    roofline = {"kernel": "bc_back_kernel (M <- Q_b M)", "bound": "tensor",
+                "achieved": round(achieved, 3), "peak": round(fp64_peak, 3), "unit": "TFLOP/s",
+                "frac": round(achieved / fp64_peak, 4), "traffic": traffic,
+                "peak_source": "FP64: cuBLAS DGEMM 8192^3 measured in this run (no FP64 figure "
+                               "in MEASURED_PEAKS.json)",
+                "algorithmic_flop_per_launch": bcb_flops}
+
+    if rank == 0:
+        cpu = None
+        if not args.no_cpu:
+            v_cpu, t_cpu = cpu_oracle_sample(args.cpu_n)
+            v_lap, t_lap = lapack_dsyevd_sample(args.cpu_n)
+            cpu = {"value": round(v_cpu, 6), "unit": "TFLOP/s", "cores": os.cpu_count(),
+                   "kind": "port",
+                   "sample": f"one oracle solve (reference pipeline on the CPU) at n={args.cpu_n}"
+                             f": {t_cpu:.2f} s; BLAS calls threaded over the host cores, bulge "
+                             "chase and LAPACK D&C pieces sequential",
+                   "lapack_dsyevd": {"value": round(v_lap, 6), "unit": "TFLOP/s",
+                                     "seconds": round(t_lap, 3), "n": args.cpu_n}}
+        line = {
+            "metric": metric_name(n), "value": round(value, 4), "unit": "TFLOP/s",
+            "n_gpus": world, "steps": args.steps, "warmup": max(3, args.warmup),
+            "ms_per_step": round(ms_per, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"eigh n={n}: A=(G+G^T)/2, G iid N(0,1), FP64 form, "
+                                   "all eigenvalues and eigenvectors",
+                       "n": n, "nbw": args.nbw or "default", "nk": args.nk or "default",
+                       "parallelism": f"replicas x{world}",
+                       "l2": "inputs (2.1 GB per matrix) exceed the 126 MB L2; no flush"},
+            "stage_ms": {k2: round(v, 3) for k2, v in med.items()},
+            "tflops_ref_convention": round(world * args.steps * (4.0 / 3.0) * n ** 3
+                                           / (total_ms * 1e-3) / 1e12, 4),
+            "accuracy": {"resid_n_norm2": resid, "resid_fro_rel": resid_ref, "orth_fro": orth},
+            "gpu_launches": int(launches),
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["cuev", "reference"], default="cuev")
+    ap.add_argument("--n", type=int, default=16384)
+    ap.add_argument("--nbw", type=int, default=0)
+    ap.add_argument("--nk", type=int, default=0)
+    ap.add_argument("--cpu-n", type=int, default=2048)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args(argv)
+    rank = _env_int("RANK", 0)
+    world = _env_int("WORLD_SIZE", 1)
+    local_rank = _env_int("LOCAL_RANK", 0)
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    return run_cuev(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -265,36 +265,32 @@ def _laex3(k, n, n1, d, Q, ldq, qoff, rho, dlamda, Q2, indx, ctot, w):
         if info != 0:
             raise RuntimeError(f"dlaed4 failed, info = {info}")
         d[j] = lam
-    Qv = lambda i, j: Q[qoff + i + j * ldq]  # noqa: E731
+    def block(rows, cols):  # Fortran view of Q's leading rows x cols block
+        return np.lib.stride_tricks.as_strided(Q[qoff:], shape=(rows, cols),
+                                               strides=(8, 8 * ldq))
+
     if k == 2:
-        for j in range(2):
-            t = [Qv(0, j), Qv(1, j)]
-            Q[qoff + 0 + j * ldq] = t[indx[0] - 1]
-            Q[qoff + 1 + j * ldq] = t[indx[1] - 1]
+        Dk = block(2, 2)
+        t = Dk.copy()
+        Dk[0, :] = t[indx[0] - 1, :]
+        Dk[1, :] = t[indx[1] - 1, :]
     elif k != 1:
-        D = np.array([[Qv(i, j) for j in range(k)] for i in range(k)])  # deltas, D[i, j]
-        s = w[:k].copy()
-        wn = np.empty(k)
+        D = block(k, k).copy()  # deltas, D[i, j] = dlamda_i - lambda_j
         dl = dlamda[:k]
-        for i in range(k):
-            wi = D[i, i]
-            for j in range(k):
-                if j != i:
-                    wi *= D[i, j] / (dl[i] - dl[j])
-            wn[i] = np.copysign(np.sqrt(-wi), s[i])
+        ratio = D / np.where(np.eye(k, dtype=bool), 1.0, dl[:, None] - dl[None, :])
+        np.fill_diagonal(ratio, 1.0)
+        wi = np.diag(D) * np.prod(ratio, axis=1)
+        wn = np.copysign(np.sqrt(-wi), w[:k])
         w[:k] = wn
         S = wn[:, None] / D
         S /= np.linalg.norm(S, axis=0)[None, :]
         perm = np.asarray(indx[:k]) - 1
-        S = S[perm, :]
-        for j in range(k):
-            for i in range(k):
-                Q[qoff + i + j * ldq] = S[i, j]
+        block(k, k)[:, :] = S[perm, :]
     n2 = n - n1
     n12 = ctot[0] + ctot[1]
     n23 = ctot[1] + ctot[2]
     iq2 = n1 * n12
-    Sm = np.array([[Q[qoff + i + j * ldq] for j in range(k)] for i in range(k)])
+    Sm = block(k, k).copy()
     out2 = None
     if n23 != 0:
         Q2b = Q2[iq2:iq2 + n2 * n23].reshape((n2, n23), order="F")
@@ -303,10 +299,9 @@ def _laex3(k, n, n1, d, Q, ldq, qoff, rho, dlamda, Q2, indx, ctot, w):
     if n12 != 0:
         Q2a = Q2[:n1 * n12].reshape((n1, n12), order="F")
         out1 = Q2a @ Sm[:n12, :]
-    for j in range(k):
-        col = qoff + j * ldq
-        Q[col + n1:col + n] = out2[:, j] if out2 is not None else 0.0
-        Q[col:col + n1] = out1[:, j] if out1 is not None else 0.0
+    blk = block(n, k)
+    blk[n1:n, :] = out2 if out2 is not None else 0.0
+    blk[0:n1, :] = out1 if out1 is not None else 0.0
 
 
 def _laex1(n, d, doff, Q, ldq, qoff, indxq, ioff, rho, cutpnt, work):
@@ -383,13 +378,9 @@ def _laex0(n, d, e, off, Q, ldq, indxq):
     # reorder columns by indxq (ascending eigenvalues)
     perm = indxq[off:off + n] - 1
     dd = d[off:off + n][perm].copy()
-    blk = np.empty((n, n))
-    for i in range(n):
-        c = off + perm[i]
-        blk[:, i] = Q[(off + c * ldq):(off + c * ldq + n)]
+    view = np.lib.stride_tricks.as_strided(Q[off + off * ldq:], shape=(n, n), strides=(8, 8 * ldq))
+    view[:, :] = view[:, perm].copy()
     d[off:off + n] = dd
-    for i in range(n):
-        Q[(off + (off + i) * ldq):(off + (off + i) * ldq + n)] = blk[:, i]
 
 
 def tridi_dc(d_in: np.ndarray, e_in: np.ndarray):
