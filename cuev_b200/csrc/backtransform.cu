@@ -28,97 +28,169 @@
 namespace cuev {
 namespace {
 
-template <int BW, int TS> struct BcBackCfg {
-    static constexpr int R = TS + BW - 1; // register rows per column
-};
+__device__ __forceinline__ void cp_async8(double *smem, const double *gmem, bool pred) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gmem),
+                 "r"(pred ? 8 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N> __device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+// 16-byte shared load of two reflector entries (broadcast: every lane reads the same address).
+// Plain loads let the compiler re-read w for the update instead of keeping it live (volatile
+// asm loads made it hoist them and spill).
+__device__ __forceinline__ double2 lds2(const double *p) {
+    return *reinterpret_cast<const double2 *>(p);
+}
 
-// One thread = one column of M.  NWARP warps per CTA.
+// One thread = one column of M; NWARP warps per CTA.  Shared memory (doubles):
+//   sW  [2][TS][BW]       static: reflectors of the current and the next hop block (cp.async)
+//   sIn [NT][BW+2]        dynamic: incoming rows of M for the next step (cp.async, coalesced)
+//   sOut[NT][BW+2]        dynamic: finished rows of M, stored cooperatively (coalesced)
+// The register window m[] is only ever indexed with compile-time constants and only exchanges
+// data with shared memory, which keeps it at 95 doubles without spills.
+template <int BW, int TS> constexpr size_t bc_back_smem(int nt) {
+    return sizeof(double) * (2 * (size_t)nt * (BW + 2));
+}
+
 template <int BW, int TS, int NWARP>
 __global__ void __launch_bounds__(32 * NWARP)
     bc_back_kernel(const double *__restrict__ U, long long ldu, double *__restrict__ M,
                    long long ldm, int n, int ncols) {
-    constexpr int R = BcBackCfg<BW, TS>::R;
-    __shared__ __align__(16) double sW[TS][BW]; // reflectors of the current hop block
-    const int col = blockIdx.x * (32 * NWARP) + threadIdx.x;
-    const bool active = col < ncols;
-    double *__restrict__ Mc = M + (long long)(active ? col : 0) * ldm;
+    constexpr int NT = 32 * NWARP;
+    constexpr int R = TS + BW - 1; // register rows per column
+    constexpr int KEEP = TS - 1;   // rows carried from one hop block to the next
+    constexpr int MLD = BW + 2;    // 16-byte multiple, conflict-free 16-byte accesses
+    // reflectors in a static array: with an extern (dynamic) base the compiler spills the window
+    __shared__ __align__(16) double sW[2 * TS * BW];
+    extern __shared__ __align__(16) double bsm[];
+    double *sIn = bsm;
+    double *sOut = bsm + NT * MLD;
+    const int tid = threadIdx.x;
+    const int col0 = blockIdx.x * NT;
     const int nsweeps = n - 2;
     if (nsweeps <= 0) return;
 
+    // reflectors (s0 + t, h): rows [base + t, base + t + BW) of U[:, s0 + t]
+    auto stage_w = [&](int buf, int s0, int base) {
+        double *dst = sW + buf * TS * BW;
+#pragma unroll 4
+        for (int idx = tid; idx < TS * BW; idx += NT) {
+            const int t = idx / BW, i = idx % BW;
+            const int s = s0 + t, row = base + t + i;
+            const bool ok = (s < nsweeps) && (row < n);
+            cp_async8(dst + idx, ok ? U + row + (long long)s * ldu : U, ok);
+        }
+    };
+    // rows [row0, row0 + BW) of the CTA's columns -> sIn, coalesced along rows
+    auto stage_in = [&](int row0) {
+#pragma unroll 4
+        for (int idx = tid; idx < NT * BW; idx += NT) {
+            const int i = idx % BW, c = idx / BW;
+            const int row = row0 + i, cc = col0 + c;
+            const bool ok = (cc < ncols) && (row < n);
+            cp_async8(sIn + c * MLD + i, ok ? M + row + (long long)cc * ldm : M, ok);
+        }
+    };
+    // sOut -> rows [row0, row0 + cnt) of the CTA's columns
+    auto store_out = [&](int row0, int cnt) {
+        for (int idx = tid; idx < NT * BW; idx += NT) {
+            const int i = idx % BW, c = idx / BW;
+            const int row = row0 + i, cc = col0 + c;
+            if (i < cnt && cc < ncols && row < n) M[row + (long long)cc * ldm] = sOut[c * MLD + i];
+        }
+    };
+
     double m[R];
     const int ntile = (nsweeps + TS - 1) / TS;
+    const int mycol = min(col0 + tid, ncols - 1); // clamped: out-of-range lanes compute garbage
+    const bool active = col0 + tid < ncols;      // ... and never store it
+    const double *Mc = M + (long long)mycol * ldm;
     for (int tile = ntile - 1; tile >= 0; --tile) {
         const int s0 = tile * TS;
-        const int top = s0 + 1; // first row touched by the tile
+        const int top = s0 + 1;              // first row touched by the tile
         const int hmax = (n - 1 - top) / BW; // last hop block with rows inside the matrix
-        // initial window: rows [top, top + R)
+        __syncthreads();
+        stage_w(0, s0, top);
+        stage_in(top + KEEP);
+        cp_async_commit();
+        // carried rows of the first step: [top, top + KEEP), rows past n read as 0
 #pragma unroll
-        for (int i = 0; i < R; ++i) {
+        for (int i = 0; i < KEEP; ++i) {
             const int row = top + i;
-            m[i] = (active && row < n) ? Mc[row] : 0.0;
+            const double v = Mc[min(row, n - 1)];
+            m[i] = row < n ? v : 0.0;
         }
         for (int h = 0; h <= hmax; ++h) {
             const int base = top + h * BW; // row of m[0]
-            __syncthreads();
-            // stage w of reflectors (s0 + t, h), rows [base + t, base + t + BW)
-            for (int idx = threadIdx.x; idx < TS * BW; idx += 32 * NWARP) {
-                const int t = idx / BW, i = idx % BW;
-                const int s = s0 + t, row = base + t + i;
-                sW[t][i] = (s < nsweeps && row < n) ? U[row + (long long)s * ldu] : 0.0;
+            cp_async_wait<0>();
+            __syncthreads(); // sW[h & 1] and sIn complete; previous sOut stored
+#pragma unroll
+            for (int i = 0; i < BW; ++i) m[KEEP + i] = sIn[tid * MLD + i];
+            __syncthreads(); // everyone has read sIn
+            if (h < hmax) {
+                stage_w((h + 1) & 1, s0, base + BW);
+                stage_in(base + BW + KEEP);
             }
-            __syncthreads();
+            cp_async_commit();
+            const double *W = sW + (h & 1) * TS * BW;
             // apply in decreasing sweep order: m[t : t+BW] -= 2 (w^T m) w
 #pragma unroll
             for (int t = TS - 1; t >= 0; --t) {
-                double d0 = 0.0, d1 = 0.0, d2 = 0.0, d3 = 0.0;
-#pragma unroll
-                for (int i = 0; i < BW; i += 4) {
-                    const double2 wa = *reinterpret_cast<const double2 *>(&sW[t][i]);
-                    const double2 wb = *reinterpret_cast<const double2 *>(&sW[t][i + 2]);
-                    d0 = fma(wa.x, m[t + i], d0);
-                    d1 = fma(wa.y, m[t + i + 1], d1);
-                    d2 = fma(wb.x, m[t + i + 2], d2);
-                    d3 = fma(wb.y, m[t + i + 3], d3);
-                }
-                const double f = -2.0 * ((d0 + d1) + (d2 + d3));
+                const double *w = W + t * BW;
+                double acc[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
 #pragma unroll
                 for (int i = 0; i < BW; i += 2) {
-                    const double2 w = *reinterpret_cast<const double2 *>(&sW[t][i]);
-                    m[t + i] = fma(f, w.x, m[t + i]);
-                    m[t + i + 1] = fma(f, w.y, m[t + i + 1]);
+                    // compiler-only fence every 32 entries: keeps at most 32 w values in flight
+                    if (i % 32 == 0) asm volatile("" ::: "memory");
+                    const double2 ww = lds2(w + i);
+                    acc[(i >> 1) & 3] = fma(ww.x, m[t + i], acc[(i >> 1) & 3]);
+                    acc[4 + ((i >> 1) & 3)] = fma(ww.y, m[t + i + 1], acc[4 + ((i >> 1) & 3)]);
+                }
+                const double f =
+                    -2.0 * (((acc[0] + acc[1]) + (acc[2] + acc[3])) +
+                            ((acc[4] + acc[5]) + (acc[6] + acc[7])));
+#pragma unroll
+                for (int i = 0; i < BW; i += 2) {
+                    if (i % 32 == 0) asm volatile("" ::: "memory");
+                    const double2 ww = lds2(w + i);
+                    m[t + i] = fma(f, ww.x, m[t + i]);
+                    m[t + i + 1] = fma(f, ww.y, m[t + i + 1]);
                 }
             }
-            // rows [base, base + BW) are final for this tile; shift the window down by BW
+            // rows [base, base + BW) are final for this tile; carry the rest down
 #pragma unroll
-            for (int i = 0; i < BW; ++i) {
-                const int row = base + i;
-                if (active && row < n) Mc[row] = m[i];
-            }
-            if (h < hmax) {
+            for (int i = 0; i < BW; ++i) sOut[tid * MLD + i] = m[i];
 #pragma unroll
-                for (int i = 0; i < R - BW; ++i) m[i] = m[i + BW];
+            for (int i = 0; i < KEEP; ++i) m[i] = m[i + BW];
+            __syncthreads();
+            store_out(base, BW);
+        }
+        // flush the carried rows [top + (hmax+1) BW, ... + KEEP)
+        const int fbase = top + (hmax + 1) * BW;
+        if (active) {
+            double *Mw = M + (long long)mycol * ldm;
 #pragma unroll
-                for (int i = R - BW; i < R; ++i) {
-                    const int row = base + BW + i;
-                    m[i] = (active && row < n) ? Mc[row] : 0.0;
-                }
-            } else {
-                // flush the rest of the window
-#pragma unroll
-                for (int i = BW; i < R; ++i) {
-                    const int row = base + i;
-                    if (active && row < n) Mc[row] = m[i];
-                }
-            }
+            for (int i = 0; i < KEEP; ++i)
+                if (fbase + i < n) Mw[fbase + i] = m[i];
         }
     }
 }
 
 template <int BW, int TS> int launch_bc_back(Workspace *ws, double *M, long long ldm, int ncols) {
     constexpr int NWARP = 2;
-    const int grid = div_up(ncols, 32 * NWARP);
-    bc_back_kernel<BW, TS, NWARP><<<grid, 32 * NWARP, 0, ws->stream>>>(ws->U, ws->n, M, ldm,
-                                                                       ws->n, ncols); note_launch();
+    constexpr int NT = 32 * NWARP;
+    const size_t smem = bc_back_smem<BW, TS>(NT);
+    auto kern = bc_back_kernel<BW, TS, NWARP>;
+    static bool attr = false;
+    if (!attr) {
+        CUEV_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr = true;
+    }
+    const int grid = div_up(ncols, NT);
+    kern<<<grid, NT, smem, ws->stream>>>(ws->U, ws->n, M, ldm, ws->n, ncols); note_launch();
     CUEV_TRY(cudaGetLastError());
     return CUEV_OK;
 }
@@ -127,8 +199,10 @@ template <int BW, int TS> int launch_bc_back(Workspace *ws, double *M, long long
 
 int bc_back(Workspace *ws, double *M, long long ldm) {
     if (ws->n <= 2) return CUEV_OK;
-    if (ws->b == 32) return launch_bc_back<32, 32>(ws, M, ldm, ws->n);
-    if (ws->b == 64) return launch_bc_back<64, 32>(ws, M, ldm, ws->n);
+    // register window R = TS + b - 1 rows: 79 rows keeps b = 32 spill-free (252 registers);
+    // b = 64 needs the 64 reflector entries live as well and runs a shorter tile
+    if (ws->b == 32) return launch_bc_back<32, 48>(ws, M, ldm, ws->n);
+    if (ws->b == 64) return launch_bc_back<64, 16>(ws, M, ldm, ws->n);
     return CUEV_ERR_INVALID;
 }
 

@@ -33,14 +33,17 @@ template <int BW> struct ChaseSmem {
     double S[BW][3 * BW + 1]; // strip: S[k][ii] = A(lo + ii, r0 + k)
     double w[BW];             // reflector
     double p[3 * BW];         // p = 2 A w over the window rows
-    double y[3 * BW];         // y = p - kappa w
-    double red[32];
+    double red[2];            // beta, kappa
 };
 
 template <int BW>
 __global__ void __launch_bounds__(BC_THREADS)
     bc_chase_kernel(double *__restrict__ Bp, double *__restrict__ U, long long ldu, int n, int b,
                     int *prog, int *status) {
+    constexpr int NT = BC_THREADS;
+    constexpr int NLEFT = (BW * BW + NT - 1) / NT;    // left-block elements per thread
+    constexpr int NLOW = (2 * BW * BW + NT - 1) / NT; // lower-part elements per thread
+    constexpr int NUPD = (3 * BW * BW + NT - 1) / NT; // strip elements per thread
     extern __shared__ __align__(16) unsigned char smem_raw[];
     ChaseSmem<BW> &sm = *reinterpret_cast<ChaseSmem<BW> *>(smem_raw);
     const int tid = threadIdx.x;
@@ -88,26 +91,46 @@ __global__ void __launch_bounds__(BC_THREADS)
             if (s_abort) return;
             __threadfence();
 
-            // ---- gather the strip S[k][ii] = A(lo+ii, r0+k): rows above r0 (left block)
-            // are stored in packed columns i (contiguous along k), the rest in packed column j.
-            for (int idx = tid; idx < off * L; idx += BC_THREADS) {
-                const int k = idx % L, ii = idx / L;
+            // ---- gather the strip S[k][ii] = A(lo+ii, r0+k), all loads in flight at once.
+            // left block (rows above r0): packed column i, contiguous along k
+            double vl[NLEFT], vw[NLOW];
+#pragma unroll
+            for (int q = 0; q < NLEFT; ++q) {
+                const int idx = tid + q * NT;
+                const int k = idx % BW, ii = idx / BW;
+                const bool ok = (ii < off) && (k < L);
                 const int i = lo + ii, j = r0 + k;
-                sm.S[k][ii] = __ldcg(&Bp[(j - i) + (long long)i * ldb]);
+                vl[q] = ok ? __ldcg(&Bp[(j - i) + (long long)i * ldb]) : 0.0;
             }
-            for (int idx = tid; idx < (W - off) * L; idx += BC_THREADS) {
-                const int ii = off + idx % (W - off), k = idx / (W - off);
+            // rows r0..hi: packed column j (lower triangle only; the upper half of the
+            // diagonal block follows by symmetry)
+#pragma unroll
+            for (int q = 0; q < NLOW; ++q) {
+                const int idx = tid + q * NT;
+                const int ii = off + idx % (2 * BW), k = idx / (2 * BW);
                 const int i = lo + ii, j = r0 + k;
-                if (i >= j) sm.S[k][ii] = __ldcg(&Bp[(i - j) + (long long)j * ldb]);
+                const bool ok = (ii < W) && (k < L) && (i >= j);
+                vw[q] = ok ? __ldcg(&Bp[(i - j) + (long long)j * ldb]) : 0.0;
+            }
+#pragma unroll
+            for (int q = 0; q < NLEFT; ++q) {
+                const int idx = tid + q * NT;
+                const int k = idx % BW, ii = idx / BW;
+                if (ii < off && k < L) sm.S[k][ii] = vl[q];
+            }
+#pragma unroll
+            for (int q = 0; q < NLOW; ++q) {
+                const int idx = tid + q * NT;
+                const int ii = off + idx % (2 * BW), k = idx / (2 * BW);
+                const int i = lo + ii, j = r0 + k;
+                if (ii < W && k < L && i >= j) sm.S[k][ii] = vw[q];
             }
             __syncthreads();
-            // upper part of the diagonal block by symmetry
-            for (int idx = tid; idx < L * L; idx += BC_THREADS) {
-                const int a = idx % L, k = idx / L; // row r0+a, column r0+k, a < k
-                if (a < k) sm.S[k][off + a] = sm.S[a][off + k];
+            // upper part of the diagonal block by symmetry; Householder of x = S[0:L][0]
+            for (int idx = tid; idx < BW * BW; idx += NT) {
+                const int a = idx % BW, k = idx / BW; // row r0+a, column r0+k
+                if (a < k && k < L) sm.S[k][off + a] = sm.S[a][off + k];
             }
-
-            // ---- Householder of x = A(r0:r1, cq) = S[0:L][0]
             if (warp == 0) {
                 double ss = 0.0;
                 for (int k = lane; k < L; k += 32) {
@@ -131,61 +154,66 @@ __global__ void __launch_bounds__(BC_THREADS)
             __syncthreads();
 
             // ---- p = 2 A w over the window rows
-            for (int ii = tid; ii < W; ii += BC_THREADS) {
-                double acc = 0.0;
-#pragma unroll 8
-                for (int k = 0; k < L; ++k) acc += sm.S[k][ii] * sm.w[k];
-                sm.p[ii] = 2.0 * acc;
+            for (int ii = tid; ii < W; ii += NT) {
+                double a0 = 0.0, a1 = 0.0;
+                int k = 0;
+                for (; k + 1 < L; k += 2) {
+                    a0 = fma(sm.S[k][ii], sm.w[k], a0);
+                    a1 = fma(sm.S[k + 1][ii], sm.w[k + 1], a1);
+                }
+                if (k < L) a0 = fma(sm.S[k][ii], sm.w[k], a0);
+                sm.p[ii] = 2.0 * (a0 + a1);
             }
             __syncthreads();
-            // kappa = w^T p (over the reflector rows)
-            if (warp == 0) {
-                double kl = 0.0;
-                for (int k = lane; k < L; k += 32) kl += sm.w[k] * sm.p[off + k];
-                kl = warp_sum(kl);
-                if (lane == 0) sm.red[1] = kl;
-            }
-            __syncthreads();
-            const double kappa = sm.red[1];
-            for (int ii = tid; ii < W; ii += BC_THREADS) {
-                const int k = ii - off;
-                const double wr = (k >= 0 && k < L) ? sm.w[k] : 0.0;
-                sm.y[ii] = sm.p[ii] - kappa * wr;
-            }
-            __syncthreads();
+            // kappa = w^T p over the reflector rows (every warp computes it)
+            double kl = 0.0;
+            for (int k = lane; k < L; k += 32) kl += sm.w[k] * sm.p[off + k];
+            const double kappa = warp_sum(kl);
+            const double beta = sm.red[0];
 
-            // ---- rank-2 update of the strip: S -= w_row y_col^T + y_row w_col^T
-            for (int idx = tid; idx < W * L; idx += BC_THREADS) {
-                const int ii = idx % W, k = idx / W;
+            // ---- rank-2 update S -= w_row y_col^T + y_row w_col^T with y = p - kappa w;
+            // the reduced column is set exactly: A(r0, cq) = beta, A(r0+1:r1, cq) = 0
+#pragma unroll 4
+            for (int q = 0; q < NUPD; ++q) {
+                const int idx = tid + q * NT;
+                const int ii = idx % (3 * BW), k = idx / (3 * BW);
+                if (ii >= W || k >= L) continue;
+                if (ii == 0) {
+                    sm.S[k][0] = (k == 0) ? beta : 0.0;
+                    continue;
+                }
                 const int kr = ii - off;
                 const double wr = (kr >= 0 && kr < L) ? sm.w[kr] : 0.0;
-                sm.S[k][ii] -= wr * sm.y[off + k] + sm.y[ii] * sm.w[k];
+                const double wk = sm.w[k];
+                const double yr = sm.p[ii] - kappa * wr;
+                const double yc = sm.p[off + k] - kappa * wk;
+                sm.S[k][ii] -= wr * yc + yr * wk;
             }
-            __syncthreads();
-            // the reduced column is exact: A(r0, cq) = beta, A(r0+1:r1, cq) = 0
-            if (tid < L) sm.S[tid][0] = (tid == 0) ? sm.red[0] : 0.0;
             __syncthreads();
 
-            // ---- scatter back (lower triangle of the strip, and the left block)
-            for (int idx = tid; idx < off * L; idx += BC_THREADS) {
-                const int k = idx % L, ii = idx / L;
-                const int i = lo + ii, j = r0 + k;
-                __stcg(&Bp[(j - i) + (long long)i * ldb], sm.S[k][ii]);
+            // ---- scatter back (left block and lower triangle) and store the reflector
+#pragma unroll
+            for (int q = 0; q < NLEFT; ++q) {
+                const int idx = tid + q * NT;
+                const int k = idx % BW, ii = idx / BW;
+                if (ii < off && k < L) {
+                    const int i = lo + ii, j = r0 + k;
+                    __stcg(&Bp[(j - i) + (long long)i * ldb], sm.S[k][ii]);
+                }
             }
-            for (int idx = tid; idx < (W - off) * L; idx += BC_THREADS) {
-                const int ii = off + idx % (W - off), k = idx / (W - off);
+#pragma unroll
+            for (int q = 0; q < NLOW; ++q) {
+                const int idx = tid + q * NT;
+                const int ii = off + idx % (2 * BW), k = idx / (2 * BW);
                 const int i = lo + ii, j = r0 + k;
-                if (i >= j) __stcg(&Bp[(i - j) + (long long)j * ldb], sm.S[k][ii]);
+                if (ii < W && k < L && i >= j) __stcg(&Bp[(i - j) + (long long)j * ldb], sm.S[k][ii]);
             }
-            // reflector -> U[r0:r1, s]
-            for (int k = tid; k < L; k += BC_THREADS) U[(r0 + k) + (long long)s * ldu] = sm.w[k];
+            for (int k = tid; k < L; k += NT) U[(r0 + k) + (long long)s * ldu] = sm.w[k];
 
-            // ---- publish (release)
+            // ---- publish (release): every thread's stores are ordered before the flag
+            __threadfence();
             __syncthreads();
-            if (tid == 0) {
-                __threadfence();
-                st_release(&prog[s], cq);
-            }
+            if (tid == 0) st_release(&prog[s], cq);
         }
         if (tid == 0) {
             __threadfence();

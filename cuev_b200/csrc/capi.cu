@@ -25,10 +25,13 @@ struct CachedWs {
 std::mutex g_cache_mu;
 CachedWs g_cache[64];
 
-int default_b(int n) { return n >= 4096 ? 64 : 32; }
-int default_k(int n, int b) {
+int default_b(int n) {
     (void)n;
-    return b == 64 ? 512 : 256;
+    return 32;
+}
+int default_k(int n, int b) {
+    (void)b;
+    return n >= 8192 ? 512 : 256;
 }
 
 int acquire_ws(int n, int b, int k, cudaStream_t stream, Workspace **out, bool *cached) {
