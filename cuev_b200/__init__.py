@@ -78,6 +78,7 @@ _SIGS = {
     "cuev_sbr_back": [_VP, _DP, _I],
     "cuev_back_transform": [_VP, _DP, C.POINTER(Timer)],
     "cuev_dgemm": [_VP, _I, _I, _I, _I, _I, _D, _DP, _I, _DP, _I, _D, _DP, _I],
+    "cuev_dgemm_noalloc": [_VP, _I, _I, _I, _I, _I, _D, _DP, _I, _DP, _I, _D, _DP, _I],
     "cuev_dsymm_lower": [_VP, _I, _I, _D, _DP, _I, _DP, _I, _D, _DP, _I],
     "cuev_dsyr2k_lower": [_VP, _I, _I, _D, _DP, _I, _DP, _I, _D, _DP, _I],
     "cuev_dsyevd_mixed": [_DP, _I, _DP, _DP, _I, _D, _VP, C.POINTER(RefineInfo)],
@@ -275,6 +276,13 @@ def _wrap_device(ptr: int, numel: int, dtype):
 def dgemm(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, Cm, ldc, stream=None):
     _check(lib().cuev_dgemm(_stream(stream), int(ta), int(tb), m, n, k, alpha, _ptr(A), lda,
                             _ptr(B), ldb, beta, _ptr(Cm), ldc), "cuev_dgemm")
+
+
+def dgemm_noalloc(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, Cm, ldc, stream=None):
+    """``cuev_dgemm`` without any device allocation (split-K partials in the library's fixed
+    16 MiB array; m * n <= 1048576; concurrent calls race)."""
+    _check(lib().cuev_dgemm_noalloc(_stream(stream), int(ta), int(tb), m, n, k, alpha, _ptr(A),
+                                    lda, _ptr(B), ldb, beta, _ptr(Cm), ldc), "cuev_dgemm_noalloc")
 
 
 def dsymm_lower(m, n, alpha, A, lda, B, ldb, beta, Cm, ldc, stream=None):

@@ -145,6 +145,22 @@ int cuev_back_transform(cuev_handle h, double *evec, cuev_timer *timer);
 int cuev_dgemm(void *stream, int ta, int tb, int m, int n, int k, double alpha, const double *A,
                int lda, const double *B, int ldb, double beta, double *C, int ldc);
 
+/* Same product as cuev_dgemm, for callers that cannot allocate device memory.  No counterpart in
+ * the reference.  cuev_dgemm takes its split-K partial-sum buffer from cudaMalloc; a caller whose
+ * device memory is owned by its framework's caching allocator, or that must not block on a
+ * device allocation (latency-critical serving loops), can use this entry instead: it allocates
+ * nothing and keeps the partial sums in a fixed 16 MiB array inside the library (held on every
+ * GPU that loads the library until the process exits).
+ *   - Limit: m * n <= 1048576; larger problems return CUEV_ERR_INVALID (use cuev_dgemm).
+ *   - The first call on a device looks up the array's device address (cudaGetSymbolAddress);
+ *     make that first call before any stream capture on that device.
+ *   - All calls share the array: calls that overlap on the GPU (other streams, other host
+ *     threads) race and give wrong results; serialise them.  Every partial sum is written by the
+ *     call before it is read, so no clearing is needed between calls. */
+int cuev_dgemm_noalloc(void *stream, int ta, int tb, int m, int n, int k, double alpha,
+                       const double *A, int lda, const double *B, int ldb, double beta, double *C,
+                       int ldc);
+
 /* C = alpha A B + beta C with A symmetric (m x m, lower triangle read).  Replaces
  * cuev::cublas::symm(LEFT, LOWER) (reference src/cuda/cublas.cu:28-37). */
 int cuev_dsymm_lower(void *stream, int m, int n, double alpha, const double *A, int lda,
