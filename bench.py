@@ -47,6 +47,21 @@ def metric_name(n):
     return f"eigh n={n} FP64 (all eigenpairs), TFLOP/s at 6.67 n^3 per solve"
 
 
+def max_over_ranks(value: float, dist=None, device=None) -> float:
+    """Max of a per-rank timing over all ranks (replicas: the job ends with the slowest)."""
+    if dist is None:
+        return float(value)
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_tflops(world: int, steps: int, n: int, total_ms: float) -> float:
+    """Aggregate throughput of `world` replicas each doing `steps` solves of size n."""
+    return world * steps * FLOP_MODEL * n ** 3 / (total_ms * 1e-3) / 1e12
+
+
 # ------------------------------------------------------------------------------------------
 # clocks sampled during the timed region
 # ------------------------------------------------------------------------------------------
@@ -256,13 +271,9 @@ def run_cuev(args, rank, world, local_rank):
     torch.cuda.synchronize()
     launches = lib.cuev_kernel_launches() - launches0
     clk = clocks.stop()
-    total_ms = sum(e0_.elapsed_time(e1_) for e0_, e1_ in ev)
-    t_max = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-    if dist:
-        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
-    total_ms = float(t_max.item())
+    total_ms = max_over_ranks(sum(e0_.elapsed_time(e1_) for e0_, e1_ in ev), dist, dev)
     ms_per = total_ms / args.steps
-    value = world * args.steps * FLOP_MODEL * n ** 3 / (total_ms * 1e-3) / 1e12
+    value = whole_job_tflops(world, args.steps, n, total_ms)
 
     # accuracy of the last solve (device, cuBLAS): ||AV - VL||_F / (n ||A||_2), ||V^T V - I||_F
     with torch.no_grad():
@@ -302,11 +313,8 @@ def run_cuev(args, rank, world, local_rank):
             x1.record(stream)
             torch.cuda.synchronize()
             tot += x0.elapsed_time(x1)
-        te = torch.tensor([tot], dtype=torch.float64, device=dev)
-        if dist:
-            dist.all_reduce(te, op=dist.ReduceOp.MAX)
-        tot = float(te.item())
-        e2e = {"value": round(world * steps_e2e * FLOP_MODEL * n ** 3 / (tot * 1e-3) / 1e12, 4),
+        tot = max_over_ranks(tot, dist, dev)
+        e2e = {"value": round(whole_job_tflops(world, steps_e2e, n, tot), 4),
                "unit": "TFLOP/s", "h2d_bytes_per_step": 8 * n * n,
                "d2h_bytes_per_step": 8 * n * n + 8 * n,
                "ms_per_step": round(tot / steps_e2e, 3)}

@@ -87,9 +87,8 @@ __global__ void __launch_bounds__(BC_THREADS)
                 }
                 s_abort = !ok;
             }
-            __syncthreads();
+            __syncthreads(); // thread 0's acquire + the barrier order the loads below
             if (s_abort) return;
-            __threadfence();
 
             // ---- gather the strip S[k][ii] = A(lo+ii, r0+k), all loads in flight at once.
             // left block (rows above r0): packed column i, contiguous along k
@@ -210,8 +209,8 @@ __global__ void __launch_bounds__(BC_THREADS)
             }
             for (int k = tid; k < L; k += NT) U[(r0 + k) + (long long)s * ldu] = sm.w[k];
 
-            // ---- publish (release): every thread's stores are ordered before the flag
-            __threadfence();
+            // ---- publish: the barrier orders every thread's stores before thread 0's release
+            // (release is cumulative over what thread 0 has observed through the barrier)
             __syncthreads();
             if (tid == 0) st_release(&prog[s], cq);
         }

@@ -21,11 +21,19 @@ template <int BM_, int BN_, int WARPS_M_, int WARPS_N_, int STAGES_> struct Tile
 using CfgBig = TileCfg<128, 128, 2, 4, 3>;
 using CfgSkinny = TileCfg<128, 64, 4, 2, 4>;
 using CfgSmall = TileCfg<64, 64, 2, 2, 4>;
+using CfgN32 = TileCfg<256, 32, 8, 1, 4>; // N <= 32 (band width 32 panels)
 
 __device__ __forceinline__ void cp_async8(double *smem, const double *gmem, bool pred) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
     const int sz = pred ? 8 : 0; // src-size 0 => zero fill, nothing is read
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(sz)
+                 : "memory");
+}
+// 16-byte copy; src_bytes in {0, 8, 16}, the rest of the 16 bytes is zero-filled
+__device__ __forceinline__ void cp_async16(double *smem, const double *gmem, int src_bytes) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem),
+                 "r"(src_bytes)
                  : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
@@ -53,7 +61,10 @@ template <class C, bool TA, bool TB, bool SYMM> struct SmemLayout {
     static constexpr size_t BYTES = (size_t)C::STAGES * STAGE_ELEMS * sizeof(double);
 };
 
-template <class C, bool TA, bool TB, bool SYMM, bool BATCHED>
+// VEC = 2: global tiles are read as 16-byte pairs along their contiguous dimension (needs
+// 16-byte aligned bases, even leading dimensions and an even first K segment); VEC = 1 reads
+// single elements and accepts any alignment.
+template <class C, bool TA, bool TB, bool SYMM, bool BATCHED, int VEC>
 __global__ void __launch_bounds__(C::NT)
     dgemm_kernel(const GemmArgs args_val, const GemmArgs *__restrict__ args_arr) {
     using L = SmemLayout<C, TA, TB, SYMM>;
@@ -89,6 +100,57 @@ __global__ void __launch_bounds__(C::NT)
     const int wn0 = (warp / C::WARPS_M) * C::WN;
 
     auto load_stage = [&](int slot, int k0) {
+        if (VEC == 2 && !SYMM) {
+            double *sA = smem + slot * L::STAGE_ELEMS;
+            double *sB = sA + L::A_ELEMS;
+            if (L::A_OUTER) { // A contiguous along m
+#pragma unroll
+                for (int it = 0; it < (C::BM / 2) * BK / C::NT; ++it) {
+                    const int e = tid + it * C::NT;
+                    const int r = 2 * (e % (C::BM / 2)), kk = e / (C::BM / 2);
+                    const int i = bm + r, kg = k0 + kk;
+                    const int nb = (i < m && kg < kend) ? (i + 1 < m ? 16 : 8) : 0;
+                    const double *src = A;
+                    if (nb) src = (kg < k1) ? A + i + (long long)kg * lda : A2 + i + (long long)(kg - k1) * lda2;
+                    cp_async16(sA + kk * (C::BM + PAD) + r, src, nb);
+                }
+            } else { // A^T: contiguous along k
+#pragma unroll
+                for (int it = 0; it < C::BM * (BK / 2) / C::NT; ++it) {
+                    const int e = tid + it * C::NT;
+                    const int kk = 2 * (e % (BK / 2)), r = e / (BK / 2);
+                    const int i = bm + r, kg = k0 + kk;
+                    const int nb = (i < m && kg < kend) ? (kg + 1 < kend ? 16 : 8) : 0;
+                    const double *src = A;
+                    if (nb) src = (kg < k1) ? A + kg + (long long)i * lda : A2 + (kg - k1) + (long long)i * lda2;
+                    cp_async16(sA + r * (BK + PAD) + kk, src, nb);
+                }
+            }
+            if (L::B_OUTER) { // B^T: contiguous along n
+#pragma unroll
+                for (int it = 0; it < (C::BN / 2) * BK / C::NT; ++it) {
+                    const int e = tid + it * C::NT;
+                    const int c = 2 * (e % (C::BN / 2)), kk = e / (C::BN / 2);
+                    const int j = bn + c, kg = k0 + kk;
+                    const int nb = (j < n && kg < kend) ? (j + 1 < n ? 16 : 8) : 0;
+                    const double *src = B;
+                    if (nb) src = (kg < k1) ? B + j + (long long)kg * ldb : B2 + j + (long long)(kg - k1) * ldb2;
+                    cp_async16(sB + kk * (C::BN + PAD) + c, src, nb);
+                }
+            } else { // B: contiguous along k
+#pragma unroll
+                for (int it = 0; it < C::BN * (BK / 2) / C::NT; ++it) {
+                    const int e = tid + it * C::NT;
+                    const int kk = 2 * (e % (BK / 2)), c = e / (BK / 2);
+                    const int j = bn + c, kg = k0 + kk;
+                    const int nb = (j < n && kg < kend) ? (kg + 1 < kend ? 16 : 8) : 0;
+                    const double *src = B;
+                    if (nb) src = (kg < k1) ? B + kg + (long long)j * ldb : B2 + (kg - k1) + (long long)j * ldb2;
+                    cp_async16(sB + c * (BK + PAD) + kk, src, nb);
+                }
+            }
+            return;
+        }
         double *sA = smem + slot * L::STAGE_ELEMS;
         double *sB = sA + L::A_ELEMS;
         // ---- A tile: op(A)[bm .. bm+BM) x [k0 .. k0+BK)
@@ -217,7 +279,15 @@ __global__ void __launch_bounds__(C::NT)
                 const int col = bn + wn0 + ni * 8 + 2 * t + (q & 1);
                 if (row >= m || col >= n) continue;
                 if (a.c_lower && row < col) continue;
-                const double v = alpha * acc[mi][ni][q];
+                double v = alpha * acc[mi][ni][q];
+                if (a.epi) {
+                    if (row == col) {
+                        v = a.epi_lambar ? a.epi_lambar[row] : 0.0;
+                    } else {
+                        const double gap = a.epi_lam[col] - a.epi_lam[row];
+                        v = (fabs(gap) < a.epi_gap) ? 0.0 : v / gap;
+                    }
+                }
                 if (W) {
                     W[row + (size_t)col * m] = v;
                 } else {
@@ -243,10 +313,10 @@ __global__ void splitk_reduce_kernel(int m, int n, int splits, const double *__r
     }
 }
 
-template <class C, bool TA, bool TB, bool SYMM, bool BATCHED>
+template <class C, bool TA, bool TB, bool SYMM, bool BATCHED, int VEC>
 int launch_cfg(const GemmArgs &a, const GemmArgs *dev_args, dim3 grid, cudaStream_t stream) {
     using L = SmemLayout<C, TA, TB, SYMM>;
-    auto kern = dgemm_kernel<C, TA, TB, SYMM, BATCHED>;
+    auto kern = dgemm_kernel<C, TA, TB, SYMM, BATCHED, VEC>;
     static bool attr_set = false; // one attribute call per instantiation and process
     if (!attr_set) {
         CUEV_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -260,17 +330,37 @@ int launch_cfg(const GemmArgs &a, const GemmArgs *dev_args, dim3 grid, cudaStrea
 
 template <class C, bool SYMM, bool BATCHED>
 int dispatch_t(const GemmArgs &a, const GemmArgs *dev_args, int ta, int tb, dim3 grid,
-               cudaStream_t stream) {
-    if (SYMM) return launch_cfg<C, false, false, true, BATCHED>(a, dev_args, grid, stream);
-    if (!ta && !tb) return launch_cfg<C, false, false, false, BATCHED>(a, dev_args, grid, stream);
-    if (!ta && tb) return launch_cfg<C, false, true, false, BATCHED>(a, dev_args, grid, stream);
-    if (ta && !tb) return launch_cfg<C, true, false, false, BATCHED>(a, dev_args, grid, stream);
-    return launch_cfg<C, true, true, false, BATCHED>(a, dev_args, grid, stream);
+               cudaStream_t stream, bool vec2 = false) {
+    if (SYMM) return launch_cfg<C, false, false, true, BATCHED, 1>(a, dev_args, grid, stream);
+    if (BATCHED) return launch_cfg<C, false, false, false, BATCHED, 1>(a, dev_args, grid, stream);
+    if (vec2) {
+        if (!ta && !tb) return launch_cfg<C, false, false, false, false, 2>(a, dev_args, grid, stream);
+        if (!ta && tb) return launch_cfg<C, false, true, false, false, 2>(a, dev_args, grid, stream);
+        if (ta && !tb) return launch_cfg<C, true, false, false, false, 2>(a, dev_args, grid, stream);
+        return launch_cfg<C, true, true, false, false, 2>(a, dev_args, grid, stream);
+    }
+    if (!ta && !tb) return launch_cfg<C, false, false, false, false, 1>(a, dev_args, grid, stream);
+    if (!ta && tb) return launch_cfg<C, false, true, false, false, 1>(a, dev_args, grid, stream);
+    if (ta && !tb) return launch_cfg<C, true, false, false, false, 1>(a, dev_args, grid, stream);
+    return launch_cfg<C, true, true, false, false, 1>(a, dev_args, grid, stream);
 }
 
-enum class Tile { Big, Skinny, Small };
+bool aligned16(const void *p) { return ((uintptr_t)p & 15) == 0; }
+
+// 16-byte loads are legal when every base is 16-byte aligned, every leading dimension is even
+// (so each column starts 16-byte aligned) and the first K segment has even length.
+bool vec2_ok(const GemmArgs &a) {
+    if (a.symm_a) return false;
+    if (!aligned16(a.A) || !aligned16(a.B) || (a.lda & 1) || (a.ldb & 1)) return false;
+    if (a.k2 > 0 && (!aligned16(a.A2) || !aligned16(a.B2) || (a.lda2 & 1) || (a.ldb2 & 1) || (a.k & 1)))
+        return false;
+    return true;
+}
+
+enum class Tile { Big, Skinny, Small, N32 };
 
 Tile pick_tile(int m, int n) {
+    if (n <= 32 && m > 64) return Tile::N32;
     if (m <= 64 && n <= 64) return Tile::Small;
     if (n <= 64 || m <= 64) return Tile::Skinny;
     return Tile::Big;
@@ -280,6 +370,7 @@ void tile_dims(Tile t, int &bm, int &bn) {
     switch (t) {
     case Tile::Big: bm = CfgBig::BM, bn = CfgBig::BN; break;
     case Tile::Skinny: bm = CfgSkinny::BM, bn = CfgSkinny::BN; break;
+    case Tile::N32: bm = CfgN32::BM, bn = CfgN32::BN; break;
     default: bm = CfgSmall::BM, bn = CfgSmall::BN; break;
     }
 }
@@ -317,25 +408,30 @@ int gemm_launch(const GemmArgs &a_in, int ta, int tb, cudaStream_t stream) {
         CUEV_TRY(cudaGetLastError());
         return CUEV_OK;
     }
-    if (a.splits > 1 && a.ws == nullptr) a.splits = 1;
+    if ((a.splits > 1 && a.ws == nullptr) || a.epi) a.splits = 1;
     if (a.splits < 1) a.splits = 1;
     const Tile tl = pick_tile(a.m, a.n);
     int bm, bn;
     tile_dims(tl, bm, bn);
     dim3 grid(div_up(a.m, bm), div_up(a.n, bn), a.splits);
+    const bool v2 = vec2_ok(a);
     int st;
     switch (tl) {
     case Tile::Big:
         st = a.symm_a ? dispatch_t<CfgBig, true, false>(a, nullptr, 0, 0, grid, stream)
-                      : dispatch_t<CfgBig, false, false>(a, nullptr, ta, tb, grid, stream);
+                      : dispatch_t<CfgBig, false, false>(a, nullptr, ta, tb, grid, stream, v2);
         break;
     case Tile::Skinny:
         st = a.symm_a ? dispatch_t<CfgSkinny, true, false>(a, nullptr, 0, 0, grid, stream)
-                      : dispatch_t<CfgSkinny, false, false>(a, nullptr, ta, tb, grid, stream);
+                      : dispatch_t<CfgSkinny, false, false>(a, nullptr, ta, tb, grid, stream, v2);
+        break;
+    case Tile::N32:
+        st = a.symm_a ? dispatch_t<CfgN32, true, false>(a, nullptr, 0, 0, grid, stream)
+                      : dispatch_t<CfgN32, false, false>(a, nullptr, ta, tb, grid, stream, v2);
         break;
     default:
         st = a.symm_a ? dispatch_t<CfgSmall, true, false>(a, nullptr, 0, 0, grid, stream)
-                      : dispatch_t<CfgSmall, false, false>(a, nullptr, ta, tb, grid, stream);
+                      : dispatch_t<CfgSmall, false, false>(a, nullptr, ta, tb, grid, stream, v2);
         break;
     }
     if (st != CUEV_OK) return st;
@@ -352,7 +448,8 @@ int gemm_launch(const GemmArgs &a_in, int ta, int tb, cudaStream_t stream) {
 int gemm_batched_launch(const GemmArgs *dev_args, int count, int max_m, int max_n, int ta,
                         int tb, cudaStream_t stream) {
     if (count <= 0 || max_m <= 0 || max_n <= 0) return CUEV_OK;
-    const Tile tl = pick_tile(max_m, max_n);
+    Tile tl = pick_tile(max_m, max_n);
+    if (tl == Tile::N32) tl = Tile::Skinny; // batched problems use the three base tiles
     int bm, bn;
     tile_dims(tl, bm, bn);
     GemmArgs dummy{};

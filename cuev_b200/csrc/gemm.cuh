@@ -27,6 +27,12 @@ struct GemmArgs {
     int symm_a;              // 1: A is symmetric m x m, only its lower triangle is read
     double *ws;              // split-K partial sums: splits x (m x n), ld m
     int splits;
+    // Optional eigh-adjoint epilogue (m == n): C_ii = lambar_i and, for i != j,
+    // C_ij = alpha acc_ij / (lam_j - lam_i), or 0 when |lam_j - lam_i| < epi_gap.
+    // Not combined with split-K.
+    const double *epi_lam, *epi_lambar;
+    double epi_gap;
+    int epi;
 };
 
 // Host launchers (gemm.cu).  All enqueue on `stream` and return a cuev_status.

@@ -73,6 +73,18 @@ int cuev_dsyevd_cfg(double *A, int n, double *eval, double *evec, void *stream, 
  * The float input is widened and solved by the FP64 pipeline, then rounded back. */
 int cuev_ssyevd(float *A, int n, float *eval, float *evec, void *stream, cuev_timer *timer);
 
+/* Differentiation form (no reference counterpart): cotangent of A for the eigensolve,
+ *   Abar = V (diag(lambar) + sym(F o (V^T Vbar))) V^T,  F_ij = 1/(lam_j - lam_i),
+ * sym(X) = (X + X^T)/2, F_ij = 0 on the diagonal and where |lam_j - lam_i| < gap_tol (masked
+ * near-degenerate pairs).  V, Vbar, Abar are n x n column-major; lam, lambar length n; Vbar or
+ * lambar may be NULL (zero cotangent).  Only lam and V from the forward solve are needed.
+ * Enqueued on `stream`, asynchronous. */
+int cuev_dsyev_adjoint(const double *V, const double *lam, const double *Vbar,
+                       const double *lambar, int n, double gap_tol, double *Abar, void *stream);
+/* FP32 interface of the same (computed in FP64 internally). */
+int cuev_ssyev_adjoint(const float *V, const float *lam, const float *Vbar, const float *lambar,
+                       int n, float gap_tol, float *Abar, void *stream);
+
 /* Release the cached device workspace (the solves keep one pool per (n, b, k) between calls). */
 int cuev_release_workspace(void);
 
