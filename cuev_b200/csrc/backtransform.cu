@@ -55,8 +55,8 @@ template <int BW, int TS> constexpr size_t bc_back_smem(int nt) {
     return sizeof(double) * (2 * (size_t)nt * (BW + 2));
 }
 
-template <int BW, int TS, int NWARP>
-__global__ void __launch_bounds__(32 * NWARP)
+template <int BW, int TS, int NWARP, int S>
+__global__ void __launch_bounds__(32 * NWARP, 1)
     bc_back_kernel(const double *__restrict__ U, long long ldu, double *__restrict__ M,
                    long long ldm, int n, int ncols) {
     constexpr int NT = 32 * NWARP;
@@ -65,6 +65,8 @@ __global__ void __launch_bounds__(32 * NWARP)
     constexpr int MLD = BW + 2;    // 16-byte multiple, conflict-free 16-byte accesses
     // reflectors in a static array: with an extern (dynamic) base the compiler spills the window
     __shared__ __align__(16) double sW[2 * TS * BW];
+    // compact-WY factors of the S-reflector sub-blocks of the current hop block
+    __shared__ __align__(16) double sG[TS * S], sT[TS * S];
     extern __shared__ __align__(16) double bsm[];
     double *sIn = bsm;
     double *sOut = bsm + NT * MLD;
@@ -129,35 +131,82 @@ __global__ void __launch_bounds__(32 * NWARP)
             __syncthreads(); // sW[h & 1] and sIn complete; previous sOut stored
 #pragma unroll
             for (int i = 0; i < BW; ++i) m[KEEP + i] = sIn[tid * MLD + i];
-            __syncthreads(); // everyone has read sIn
+            const double *W = sW + (h & 1) * TS * BW;
+            // Gram entries G[a][b] = w_{t1+a} . w_{t1+b} (a < b) of every S-block (staircase
+            // overlap of BW - (b - a) rows)
+            for (int idx = tid; idx < TS * S; idx += NT) {
+                const int sb = idx / (S * S), a = (idx / S) % S, bb = idx % S;
+                double g = 0.0;
+                if (a < bb) {
+                    const double *wa = W + (sb * S + a) * BW + (bb - a);
+                    const double *wb = W + (sb * S + bb) * BW;
+                    for (int i = 0; i < BW - (bb - a); ++i) g = fma(wa[i], wb[i], g);
+                }
+                sG[idx] = g;
+            }
+            __syncthreads(); // everyone has read sIn; Gram ready
             if (h < hmax) {
                 stage_w((h + 1) & 1, s0, base + BW);
                 stage_in(base + BW + KEEP);
             }
             cp_async_commit();
-            const double *W = sW + (h & 1) * TS * BW;
-            // apply in decreasing sweep order: m[t : t+BW] -= 2 (w^T m) w
-#pragma unroll
-            for (int t = TS - 1; t >= 0; --t) {
-                const double *w = W + t * BW;
-                double acc[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-#pragma unroll
-                for (int i = 0; i < BW; i += 2) {
-                    // compiler-only fence every 32 entries: keeps at most 32 w values in flight
-                    if (i % 32 == 0) asm volatile("" ::: "memory");
-                    const double2 ww = lds2(w + i);
-                    acc[(i >> 1) & 3] = fma(ww.x, m[t + i], acc[(i >> 1) & 3]);
-                    acc[4 + ((i >> 1) & 3)] = fma(ww.y, m[t + i + 1], acc[4 + ((i >> 1) & 3)]);
+            // T of each S-block (H_{t1} ... H_{t1+S-1} = I - V T V^T, tau = 2):
+            // T[k][k] = 2, T[a][k] = -2 sum_{p=a}^{k-1} T[a][p] G[p][k]
+            if (tid < TS / S) {
+                const double *G = sG + tid * S * S;
+                double *Tm = sT + tid * S * S;
+                for (int k = 0; k < S; ++k) {
+                    Tm[k * S + k] = 2.0;
+                    for (int a = 0; a < k; ++a) {
+                        double acc = 0.0;
+                        for (int p = a; p < k; ++p) acc = fma(Tm[a * S + p], G[p * S + k], acc);
+                        Tm[a * S + k] = -2.0 * acc;
+                    }
+                    for (int a = k + 1; a < S; ++a) Tm[a * S + k] = 0.0;
                 }
-                const double f =
-                    -2.0 * (((acc[0] + acc[1]) + (acc[2] + acc[3])) +
-                            ((acc[4] + acc[5]) + (acc[6] + acc[7])));
+            }
+            __syncthreads();
+            // apply the hop block in decreasing sweep order, S reflectors at a time in compact-WY
+            // form: z = V^T m (S independent dot products), y = T z, m -= V y
+#pragma unroll
+            for (int sb = TS / S - 1; sb >= 0; --sb) {
+                const int t1 = sb * S;
+                const double *w0 = W + t1 * BW;
+                double z[S];
+#pragma unroll
+                for (int q = 0; q < S; ++q) z[q] = 0.0;
 #pragma unroll
                 for (int i = 0; i < BW; i += 2) {
-                    if (i % 32 == 0) asm volatile("" ::: "memory");
-                    const double2 ww = lds2(w + i);
-                    m[t + i] = fma(f, ww.x, m[t + i]);
-                    m[t + i + 1] = fma(f, ww.y, m[t + i + 1]);
+                    // __syncwarp is a compiler barrier for shared loads: it bounds the w values
+                    // the compiler keeps in flight (all lanes run this code, no divergence)
+                    if (i % 8 == 0) __syncwarp();
+#pragma unroll
+                    for (int q = 0; q < S; ++q) {
+                        const double2 ww = lds2(w0 + q * BW + i);
+                        z[q] = fma(ww.x, m[t1 + q + i], z[q]);
+                        z[q] = fma(ww.y, m[t1 + q + i + 1], z[q]);
+                    }
+                }
+                // re-read w below instead of keeping S*BW values live across y = T z
+                __syncwarp();
+                const double *Tm = sT + sb * S * S;
+                double y[S];
+#pragma unroll
+                for (int a = 0; a < S; ++a) {
+                    double acc = 0.0;
+#pragma unroll
+                    for (int q = a; q < S; ++q) acc = fma(Tm[a * S + q], z[q], acc);
+                    y[a] = acc;
+                }
+#pragma unroll
+                for (int i = 0; i < BW; i += 2) {
+                    if (i % 8 == 0) __syncwarp();
+#pragma unroll
+                    for (int q = 0; q < S; ++q) {
+                        const double2 ww = lds2(w0 + q * BW + i);
+                        m[t1 + q + i] = fma(-ww.x, y[q], m[t1 + q + i]);
+                        m[t1 + q + i + 1] = fma(-ww.y, y[q], m[t1 + q + i + 1]);
+                    }
                 }
             }
             // rows [base, base + BW) are final for this tile; carry the rest down
@@ -181,9 +230,10 @@ __global__ void __launch_bounds__(32 * NWARP)
 
 template <int BW, int TS> int launch_bc_back(Workspace *ws, double *M, long long ldm, int ncols) {
     constexpr int NWARP = 2;
+    constexpr int S = 8; // reflectors per compact-WY sub-block
     constexpr int NT = 32 * NWARP;
     const size_t smem = bc_back_smem<BW, TS>(NT);
-    auto kern = bc_back_kernel<BW, TS, NWARP>;
+    auto kern = bc_back_kernel<BW, TS, NWARP, S>;
     static bool attr = false;
     if (!attr) {
         CUEV_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -199,9 +249,9 @@ template <int BW, int TS> int launch_bc_back(Workspace *ws, double *M, long long
 
 int bc_back(Workspace *ws, double *M, long long ldm) {
     if (ws->n <= 2) return CUEV_OK;
-    // register window R = TS + b - 1 rows: 79 rows keeps b = 32 spill-free (252 registers);
-    // b = 64 needs the 64 reflector entries live as well and runs a shorter tile
-    if (ws->b == 32) return launch_bc_back<32, 48>(ws, M, ldm, ws->n);
+    // register window R = TS + b - 1 rows (63 for b = 32, 79 for b = 64) plus the S-block
+    // z, y vectors: the largest tiles that compile without spills
+    if (ws->b == 32) return launch_bc_back<32, 32>(ws, M, ldm, ws->n);
     if (ws->b == 64) return launch_bc_back<64, 16>(ws, M, ldm, ws->n);
     return CUEV_ERR_INVALID;
 }
