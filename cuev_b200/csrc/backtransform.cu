@@ -34,6 +34,10 @@ __device__ __forceinline__ void cp_async8(double *smem, const double *gmem, bool
                  "r"(pred ? 8 : 0)
                  : "memory");
 }
+__device__ __forceinline__ void cp_async16(double *smem, const double *gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 template <int N> __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
@@ -58,15 +62,15 @@ template <int BW, int TS> constexpr size_t bc_back_smem(int nt) {
 template <int BW, int TS, int NWARP, int S>
 __global__ void __launch_bounds__(32 * NWARP, 1)
     bc_back_kernel(const double *__restrict__ U, long long ldu, double *__restrict__ M,
-                   long long ldm, int n, int ncols) {
+                   long long ldm, int n, int ncols, const double *__restrict__ Tg, int nhb) {
     constexpr int NT = 32 * NWARP;
     constexpr int R = TS + BW - 1; // register rows per column
     constexpr int KEEP = TS - 1;   // rows carried from one hop block to the next
     constexpr int MLD = BW + 2;    // 16-byte multiple, conflict-free 16-byte accesses
     // reflectors in a static array: with an extern (dynamic) base the compiler spills the window
     __shared__ __align__(16) double sW[2 * TS * BW];
-    // compact-WY factors of the S-reflector sub-blocks of the current hop block
-    __shared__ __align__(16) double sG[TS * S], sT[TS * S];
+    // compact-WY factors of the S-reflector sub-blocks (current and next hop block)
+    __shared__ __align__(16) double sT[2 * TS * S];
     extern __shared__ __align__(16) double bsm[];
     double *sIn = bsm;
     double *sOut = bsm + NT * MLD;
@@ -85,6 +89,12 @@ __global__ void __launch_bounds__(32 * NWARP, 1)
             const bool ok = (s < nsweeps) && (row < n);
             cp_async8(dst + idx, ok ? U + row + (long long)s * ldu : U, ok);
         }
+    };
+    // T factors of hop block (tile, h), precomputed by bc_back_t_kernel
+    auto stage_t = [&](int buf, int tile, int h) {
+        const double *src = Tg + ((long long)tile * nhb + h) * (TS * S);
+        for (int idx = tid; idx < TS * S / 2; idx += NT)
+            cp_async16(sT + buf * TS * S + 2 * idx, src + 2 * idx);
     };
     // rows [row0, row0 + BW) of the CTA's columns -> sIn, coalesced along rows
     auto stage_in = [&](int row0) {
@@ -116,6 +126,7 @@ __global__ void __launch_bounds__(32 * NWARP, 1)
         const int hmax = (n - 1 - top) / BW; // last hop block with rows inside the matrix
         __syncthreads();
         stage_w(0, s0, top);
+        stage_t(0, tile, 0);
         stage_in(top + KEEP);
         cp_async_commit();
         // carried rows of the first step: [top, top + KEEP), rows past n read as 0
@@ -132,40 +143,13 @@ __global__ void __launch_bounds__(32 * NWARP, 1)
 #pragma unroll
             for (int i = 0; i < BW; ++i) m[KEEP + i] = sIn[tid * MLD + i];
             const double *W = sW + (h & 1) * TS * BW;
-            // Gram entries G[a][b] = w_{t1+a} . w_{t1+b} (a < b) of every S-block (staircase
-            // overlap of BW - (b - a) rows)
-            for (int idx = tid; idx < TS * S; idx += NT) {
-                const int sb = idx / (S * S), a = (idx / S) % S, bb = idx % S;
-                double g = 0.0;
-                if (a < bb) {
-                    const double *wa = W + (sb * S + a) * BW + (bb - a);
-                    const double *wb = W + (sb * S + bb) * BW;
-                    for (int i = 0; i < BW - (bb - a); ++i) g = fma(wa[i], wb[i], g);
-                }
-                sG[idx] = g;
-            }
-            __syncthreads(); // everyone has read sIn; Gram ready
+            __syncthreads(); // everyone has read sIn
             if (h < hmax) {
                 stage_w((h + 1) & 1, s0, base + BW);
+                stage_t((h + 1) & 1, tile, h + 1);
                 stage_in(base + BW + KEEP);
             }
             cp_async_commit();
-            // T of each S-block (H_{t1} ... H_{t1+S-1} = I - V T V^T, tau = 2):
-            // T[k][k] = 2, T[a][k] = -2 sum_{p=a}^{k-1} T[a][p] G[p][k]
-            if (tid < TS / S) {
-                const double *G = sG + tid * S * S;
-                double *Tm = sT + tid * S * S;
-                for (int k = 0; k < S; ++k) {
-                    Tm[k * S + k] = 2.0;
-                    for (int a = 0; a < k; ++a) {
-                        double acc = 0.0;
-                        for (int p = a; p < k; ++p) acc = fma(Tm[a * S + p], G[p * S + k], acc);
-                        Tm[a * S + k] = -2.0 * acc;
-                    }
-                    for (int a = k + 1; a < S; ++a) Tm[a * S + k] = 0.0;
-                }
-            }
-            __syncthreads();
             // apply the hop block in decreasing sweep order, S reflectors at a time in compact-WY
             // form: z = V^T m (S independent dot products), y = T z, m -= V y
 #pragma unroll
@@ -189,7 +173,7 @@ __global__ void __launch_bounds__(32 * NWARP, 1)
                 }
                 // re-read w below instead of keeping S*BW values live across y = T z
                 __syncwarp();
-                const double *Tm = sT + sb * S * S;
+                const double *Tm = sT + (h & 1) * TS * S + sb * S * S;
                 double y[S];
 #pragma unroll
                 for (int a = 0; a < S; ++a) {
@@ -228,9 +212,72 @@ __global__ void __launch_bounds__(32 * NWARP, 1)
     }
 }
 
+// T factors of every S-reflector sub-block of every hop block: one thread per (tile, h, sb).
+// Sub-block sb of hop block (tile, h) holds reflectors (s0 + t, h), t in [sb S, sb S + S), the
+// reflector t covering rows [top + h BW + t, ... + BW); H_{t1} ... H_{t1+S-1} = I - V T V^T with
+// T[k][k] = 2, T[a][k] = -2 sum_{p=a}^{k-1} T[a][p] (v_p . v_k).
+template <int BW, int TS, int S>
+__global__ void bc_back_t_kernel(const double *__restrict__ U, long long ldu, int n, int nhb,
+                                 double *__restrict__ Tg) {
+    const int ntile = (n - 2 + TS - 1) / TS;
+    const long long total = (long long)ntile * nhb * (TS / S);
+    const long long gid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (gid >= total) return;
+    const int sb = (int)(gid % (TS / S));
+    const long long th = gid / (TS / S);
+    const int h = (int)(th % nhb), tile = (int)(th / nhb);
+    const int nsweeps = n - 2;
+    const int s0 = tile * TS, base = s0 + 1 + h * BW, t1 = sb * S;
+    double G[S][S], T[S][S];
+    for (int a = 0; a < S; ++a)
+        for (int k = 0; k < S; ++k) G[a][k] = 0.0;
+    // w_{t} entry i lives at U[base + t + i, s0 + t] (zero past the matrix / past the sweeps)
+    for (int a = 0; a < S; ++a) {
+        const int sa = s0 + t1 + a;
+        if (sa >= nsweeps) continue;
+        for (int k = a + 1; k < S; ++k) {
+            const int sk = s0 + t1 + k;
+            if (sk >= nsweeps) continue;
+            double g = 0.0;
+            for (int i = 0; i + (k - a) < BW; ++i) {
+                const int row = base + t1 + k + i; // row of v_k entry i = v_a entry i + (k - a)
+                if (row >= n) break;
+                g = fma(U[row + (long long)sa * ldu], U[row + (long long)sk * ldu], g);
+            }
+            G[a][k] = g;
+        }
+    }
+    for (int k = 0; k < S; ++k) {
+        T[k][k] = 2.0;
+        for (int a = 0; a < k; ++a) {
+            double acc = 0.0;
+            for (int p = a; p < k; ++p) acc = fma(T[a][p], G[p][k], acc);
+            T[a][k] = -2.0 * acc;
+        }
+        for (int a = k + 1; a < S; ++a) T[a][k] = 0.0;
+    }
+    double *out = Tg + th * (TS * S) + sb * S * S;
+    for (int a = 0; a < S; ++a)
+        for (int k = 0; k < S; ++k) out[a * S + k] = T[a][k];
+}
+
 template <int BW, int TS> int launch_bc_back(Workspace *ws, double *M, long long ldm, int ncols) {
     constexpr int NWARP = 2;
     constexpr int S = 8; // reflectors per compact-WY sub-block
+    const int n = ws->n;
+    const int ntile = (n - 2 + TS - 1) / TS;
+    const int nhb = (n - 2) / BW + 2; // hop blocks per tile (upper bound)
+    if ((size_t)ntile * nhb * TS * S > (size_t)n * n) {
+        set_last_message("bc_back: T scratch too small");
+        return CUEV_ERR_INVALID;
+    }
+    double *Tg = ws->dc_Q2; // free during the back-transform
+    {
+        const long long total = (long long)ntile * nhb * (TS / S);
+        bc_back_t_kernel<BW, TS, S><<<(unsigned)((total + 127) / 128), 128, 0, ws->stream>>>(
+            ws->U, n, n, nhb, Tg); note_launch();
+        CUEV_TRY(cudaGetLastError());
+    }
     constexpr int NT = 32 * NWARP;
     const size_t smem = bc_back_smem<BW, TS>(NT);
     auto kern = bc_back_kernel<BW, TS, NWARP, S>;
@@ -240,7 +287,7 @@ template <int BW, int TS> int launch_bc_back(Workspace *ws, double *M, long long
         attr = true;
     }
     const int grid = div_up(ncols, NT);
-    kern<<<grid, NT, smem, ws->stream>>>(ws->U, ws->n, M, ldm, ws->n, ncols); note_launch();
+    kern<<<grid, NT, smem, ws->stream>>>(ws->U, ws->n, M, ldm, ws->n, ncols, Tg, nhb); note_launch();
     CUEV_TRY(cudaGetLastError());
     return CUEV_OK;
 }

@@ -50,6 +50,20 @@ __device__ __forceinline__ void dmma16x8x4(double (&d)[4], double a0, double a1,
                  : "d"(a0), "d"(a1), "d"(b0));
 }
 
+// D = A(16x8, row) * B(8x8, col) + D.  Fragments: a0 = A[g][t], a1 = A[g+8][t],
+//   a2 = A[g][t+4], a3 = A[g+8][t+4];  b0 = B[t][g], b1 = B[t+4][g];  D as for m16n8k4.
+__device__ __forceinline__ void dmma16x8x8(double (&d)[4], double a0, double a1, double a2,
+                                           double a3, double b0, double b1) {
+    asm volatile("mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, "
+                 "{%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+                 : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+                 : "d"(a0), "d"(a1), "d"(a2), "d"(a3), "d"(b0), "d"(b1));
+}
+
+#ifndef CUEV_DMMA_K
+#define CUEV_DMMA_K 8 // k-depth of one DMMA instruction: 4 or 8
+#endif
+
 template <class C, bool TA, bool TB, bool SYMM> struct SmemLayout {
     // "outer-contiguous" tiles are stored [k][outer] (the global matrix is contiguous along the
     // outer index), the others [outer][k].
@@ -235,6 +249,43 @@ __global__ void __launch_bounds__(C::NT)
         }
         const double *sA = smem + (kt % C::STAGES) * L::STAGE_ELEMS;
         const double *sB = sA + L::A_ELEMS;
+#if CUEV_DMMA_K == 8
+#pragma unroll
+        for (int ks = 0; ks < BK / 8; ++ks) {
+            const int kk = ks * 8 + t;
+            double af[C::MT][4], bf[C::NTL][2];
+#pragma unroll
+            for (int mi = 0; mi < C::MT; ++mi) {
+                const int r = wm0 + mi * 16 + g;
+#pragma unroll
+                for (int hh = 0; hh < 2; ++hh) { // k offset 0 / 4
+                    const int k2 = kk + 4 * hh;
+                    if (L::A_OUTER) {
+                        af[mi][2 * hh] = sA[k2 * (C::BM + PAD) + r];
+                        af[mi][2 * hh + 1] = sA[k2 * (C::BM + PAD) + r + 8];
+                    } else {
+                        af[mi][2 * hh] = sA[r * (BK + PAD) + k2];
+                        af[mi][2 * hh + 1] = sA[(r + 8) * (BK + PAD) + k2];
+                    }
+                }
+            }
+#pragma unroll
+            for (int ni = 0; ni < C::NTL; ++ni) {
+                const int c = wn0 + ni * 8 + g;
+#pragma unroll
+                for (int hh = 0; hh < 2; ++hh) {
+                    const int k2 = kk + 4 * hh;
+                    bf[ni][hh] = L::B_OUTER ? sB[k2 * (C::BN + PAD) + c] : sB[c * (BK + PAD) + k2];
+                }
+            }
+#pragma unroll
+            for (int mi = 0; mi < C::MT; ++mi)
+#pragma unroll
+                for (int ni = 0; ni < C::NTL; ++ni)
+                    dmma16x8x8(acc[mi][ni], af[mi][0], af[mi][1], af[mi][2], af[mi][3], bf[ni][0],
+                               bf[ni][1]);
+        }
+#else
 #pragma unroll
         for (int ks = 0; ks < BK / 4; ++ks) {
             const int kk = ks * 4 + t;
@@ -261,6 +312,7 @@ __global__ void __launch_bounds__(C::NT)
                 for (int ni = 0; ni < C::NTL; ++ni)
                     dmma16x8x4(acc[mi][ni], af[mi][0], af[mi][1], bf[ni]);
         }
+#endif
     }
     cp_async_wait<0>();
 
