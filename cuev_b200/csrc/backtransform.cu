@@ -34,10 +34,6 @@ __device__ __forceinline__ void cp_async8(double *smem, const double *gmem, bool
                  "r"(pred ? 8 : 0)
                  : "memory");
 }
-__device__ __forceinline__ void cp_async16(double *smem, const double *gmem) {
-    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
-}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 template <int N> __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
@@ -59,18 +55,16 @@ template <int BW, int TS> constexpr size_t bc_back_smem(int nt) {
     return sizeof(double) * (2 * (size_t)nt * (BW + 2));
 }
 
-template <int BW, int TS, int NWARP, int S>
-__global__ void __launch_bounds__(32 * NWARP, 1)
+template <int BW, int TS, int NWARP>
+__global__ void __launch_bounds__(32 * NWARP)
     bc_back_kernel(const double *__restrict__ U, long long ldu, double *__restrict__ M,
-                   long long ldm, int n, int ncols, const double *__restrict__ Tg, int nhb) {
+                   long long ldm, int n, int ncols) {
     constexpr int NT = 32 * NWARP;
     constexpr int R = TS + BW - 1; // register rows per column
     constexpr int KEEP = TS - 1;   // rows carried from one hop block to the next
     constexpr int MLD = BW + 2;    // 16-byte multiple, conflict-free 16-byte accesses
     // reflectors in a static array: with an extern (dynamic) base the compiler spills the window
     __shared__ __align__(16) double sW[2 * TS * BW];
-    // compact-WY factors of the S-reflector sub-blocks (current and next hop block)
-    __shared__ __align__(16) double sT[2 * TS * S];
     extern __shared__ __align__(16) double bsm[];
     double *sIn = bsm;
     double *sOut = bsm + NT * MLD;
@@ -89,12 +83,6 @@ __global__ void __launch_bounds__(32 * NWARP, 1)
             const bool ok = (s < nsweeps) && (row < n);
             cp_async8(dst + idx, ok ? U + row + (long long)s * ldu : U, ok);
         }
-    };
-    // T factors of hop block (tile, h), precomputed by bc_back_t_kernel
-    auto stage_t = [&](int buf, int tile, int h) {
-        const double *src = Tg + ((long long)tile * nhb + h) * (TS * S);
-        for (int idx = tid; idx < TS * S / 2; idx += NT)
-            cp_async16(sT + buf * TS * S + 2 * idx, src + 2 * idx);
     };
     // rows [row0, row0 + BW) of the CTA's columns -> sIn, coalesced along rows
     auto stage_in = [&](int row0) {
@@ -126,7 +114,6 @@ __global__ void __launch_bounds__(32 * NWARP, 1)
         const int hmax = (n - 1 - top) / BW; // last hop block with rows inside the matrix
         __syncthreads();
         stage_w(0, s0, top);
-        stage_t(0, tile, 0);
         stage_in(top + KEEP);
         cp_async_commit();
         // carried rows of the first step: [top, top + KEEP), rows past n read as 0
@@ -142,55 +129,35 @@ __global__ void __launch_bounds__(32 * NWARP, 1)
             __syncthreads(); // sW[h & 1] and sIn complete; previous sOut stored
 #pragma unroll
             for (int i = 0; i < BW; ++i) m[KEEP + i] = sIn[tid * MLD + i];
-            const double *W = sW + (h & 1) * TS * BW;
             __syncthreads(); // everyone has read sIn
             if (h < hmax) {
                 stage_w((h + 1) & 1, s0, base + BW);
-                stage_t((h + 1) & 1, tile, h + 1);
                 stage_in(base + BW + KEEP);
             }
             cp_async_commit();
-            // apply the hop block in decreasing sweep order, S reflectors at a time in compact-WY
-            // form: z = V^T m (S independent dot products), y = T z, m -= V y
+            const double *W = sW + (h & 1) * TS * BW;
+            // apply in decreasing sweep order: m[t : t+BW] -= 2 (w^T m) w
 #pragma unroll
-            for (int sb = TS / S - 1; sb >= 0; --sb) {
-                const int t1 = sb * S;
-                const double *w0 = W + t1 * BW;
-                double z[S];
-#pragma unroll
-                for (int q = 0; q < S; ++q) z[q] = 0.0;
+            for (int t = TS - 1; t >= 0; --t) {
+                const double *w = W + t * BW;
+                double acc[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
 #pragma unroll
                 for (int i = 0; i < BW; i += 2) {
-                    // __syncwarp is a compiler barrier for shared loads: it bounds the w values
-                    // the compiler keeps in flight (all lanes run this code, no divergence)
-                    if (i % 8 == 0) __syncwarp();
-#pragma unroll
-                    for (int q = 0; q < S; ++q) {
-                        const double2 ww = lds2(w0 + q * BW + i);
-                        z[q] = fma(ww.x, m[t1 + q + i], z[q]);
-                        z[q] = fma(ww.y, m[t1 + q + i + 1], z[q]);
-                    }
+                    // compiler-only fence every 32 entries: keeps at most 32 w values in flight
+                    if (i % 32 == 0) asm volatile("" ::: "memory");
+                    const double2 ww = lds2(w + i);
+                    acc[(i >> 1) & 3] = fma(ww.x, m[t + i], acc[(i >> 1) & 3]);
+                    acc[4 + ((i >> 1) & 3)] = fma(ww.y, m[t + i + 1], acc[4 + ((i >> 1) & 3)]);
                 }
-                // re-read w below instead of keeping S*BW values live across y = T z
-                __syncwarp();
-                const double *Tm = sT + (h & 1) * TS * S + sb * S * S;
-                double y[S];
-#pragma unroll
-                for (int a = 0; a < S; ++a) {
-                    double acc = 0.0;
-#pragma unroll
-                    for (int q = a; q < S; ++q) acc = fma(Tm[a * S + q], z[q], acc);
-                    y[a] = acc;
-                }
+                const double f =
+                    -2.0 * (((acc[0] + acc[1]) + (acc[2] + acc[3])) +
+                            ((acc[4] + acc[5]) + (acc[6] + acc[7])));
 #pragma unroll
                 for (int i = 0; i < BW; i += 2) {
-                    if (i % 8 == 0) __syncwarp();
-#pragma unroll
-                    for (int q = 0; q < S; ++q) {
-                        const double2 ww = lds2(w0 + q * BW + i);
-                        m[t1 + q + i] = fma(-ww.x, y[q], m[t1 + q + i]);
-                        m[t1 + q + i + 1] = fma(-ww.y, y[q], m[t1 + q + i + 1]);
-                    }
+                    if (i % 32 == 0) asm volatile("" ::: "memory");
+                    const double2 ww = lds2(w + i);
+                    m[t + i] = fma(f, ww.x, m[t + i]);
+                    m[t + i + 1] = fma(f, ww.y, m[t + i + 1]);
                 }
             }
             // rows [base, base + BW) are final for this tile; carry the rest down
@@ -212,82 +179,18 @@ __global__ void __launch_bounds__(32 * NWARP, 1)
     }
 }
 
-// T factors of every S-reflector sub-block of every hop block: one thread per (tile, h, sb).
-// Sub-block sb of hop block (tile, h) holds reflectors (s0 + t, h), t in [sb S, sb S + S), the
-// reflector t covering rows [top + h BW + t, ... + BW); H_{t1} ... H_{t1+S-1} = I - V T V^T with
-// T[k][k] = 2, T[a][k] = -2 sum_{p=a}^{k-1} T[a][p] (v_p . v_k).
-template <int BW, int TS, int S>
-__global__ void bc_back_t_kernel(const double *__restrict__ U, long long ldu, int n, int nhb,
-                                 double *__restrict__ Tg) {
-    const int ntile = (n - 2 + TS - 1) / TS;
-    const long long total = (long long)ntile * nhb * (TS / S);
-    const long long gid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (gid >= total) return;
-    const int sb = (int)(gid % (TS / S));
-    const long long th = gid / (TS / S);
-    const int h = (int)(th % nhb), tile = (int)(th / nhb);
-    const int nsweeps = n - 2;
-    const int s0 = tile * TS, base = s0 + 1 + h * BW, t1 = sb * S;
-    double G[S][S], T[S][S];
-    for (int a = 0; a < S; ++a)
-        for (int k = 0; k < S; ++k) G[a][k] = 0.0;
-    // w_{t} entry i lives at U[base + t + i, s0 + t] (zero past the matrix / past the sweeps)
-    for (int a = 0; a < S; ++a) {
-        const int sa = s0 + t1 + a;
-        if (sa >= nsweeps) continue;
-        for (int k = a + 1; k < S; ++k) {
-            const int sk = s0 + t1 + k;
-            if (sk >= nsweeps) continue;
-            double g = 0.0;
-            for (int i = 0; i + (k - a) < BW; ++i) {
-                const int row = base + t1 + k + i; // row of v_k entry i = v_a entry i + (k - a)
-                if (row >= n) break;
-                g = fma(U[row + (long long)sa * ldu], U[row + (long long)sk * ldu], g);
-            }
-            G[a][k] = g;
-        }
-    }
-    for (int k = 0; k < S; ++k) {
-        T[k][k] = 2.0;
-        for (int a = 0; a < k; ++a) {
-            double acc = 0.0;
-            for (int p = a; p < k; ++p) acc = fma(T[a][p], G[p][k], acc);
-            T[a][k] = -2.0 * acc;
-        }
-        for (int a = k + 1; a < S; ++a) T[a][k] = 0.0;
-    }
-    double *out = Tg + th * (TS * S) + sb * S * S;
-    for (int a = 0; a < S; ++a)
-        for (int k = 0; k < S; ++k) out[a * S + k] = T[a][k];
-}
-
 template <int BW, int TS> int launch_bc_back(Workspace *ws, double *M, long long ldm, int ncols) {
     constexpr int NWARP = 2;
-    constexpr int S = 8; // reflectors per compact-WY sub-block
-    const int n = ws->n;
-    const int ntile = (n - 2 + TS - 1) / TS;
-    const int nhb = (n - 2) / BW + 2; // hop blocks per tile (upper bound)
-    if ((size_t)ntile * nhb * TS * S > (size_t)n * n) {
-        set_last_message("bc_back: T scratch too small");
-        return CUEV_ERR_INVALID;
-    }
-    double *Tg = ws->dc_Q2; // free during the back-transform
-    {
-        const long long total = (long long)ntile * nhb * (TS / S);
-        bc_back_t_kernel<BW, TS, S><<<(unsigned)((total + 127) / 128), 128, 0, ws->stream>>>(
-            ws->U, n, n, nhb, Tg); note_launch();
-        CUEV_TRY(cudaGetLastError());
-    }
     constexpr int NT = 32 * NWARP;
     const size_t smem = bc_back_smem<BW, TS>(NT);
-    auto kern = bc_back_kernel<BW, TS, NWARP, S>;
+    auto kern = bc_back_kernel<BW, TS, NWARP>;
     static bool attr = false;
     if (!attr) {
         CUEV_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         attr = true;
     }
     const int grid = div_up(ncols, NT);
-    kern<<<grid, NT, smem, ws->stream>>>(ws->U, ws->n, M, ldm, ws->n, ncols, Tg, nhb); note_launch();
+    kern<<<grid, NT, smem, ws->stream>>>(ws->U, ws->n, M, ldm, ws->n, ncols); note_launch();
     CUEV_TRY(cudaGetLastError());
     return CUEV_OK;
 }
@@ -296,9 +199,9 @@ template <int BW, int TS> int launch_bc_back(Workspace *ws, double *M, long long
 
 int bc_back(Workspace *ws, double *M, long long ldm) {
     if (ws->n <= 2) return CUEV_OK;
-    // register window R = TS + b - 1 rows (63 for b = 32, 79 for b = 64) plus the S-block
-    // z, y vectors: the largest tiles that compile without spills
-    if (ws->b == 32) return launch_bc_back<32, 32>(ws, M, ldm, ws->n);
+    // register window R = TS + b - 1 rows: 79 rows keeps b = 32 spill-free (252 registers);
+    // b = 64 needs the 64 reflector entries live as well and runs a shorter tile
+    if (ws->b == 32) return launch_bc_back<32, 48>(ws, M, ldm, ws->n);
     if (ws->b == 64) return launch_bc_back<64, 16>(ws, M, ldm, ws->n);
     return CUEV_ERR_INVALID;
 }
