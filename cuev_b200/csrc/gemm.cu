@@ -2,6 +2,7 @@
 #include "gemm.cuh"
 
 #include <algorithm>
+#include <type_traits>
 
 namespace cuev {
 namespace {
@@ -41,16 +42,7 @@ template <int N> __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-// D = A(16x4, row) * B(4x8, col) + D.  Fragment ownership (g = lane/4, t = lane%4):
-//   a0 = A[g][t], a1 = A[g+8][t];  b0 = B[t][g];  d0,d1 = D[g][2t,2t+1], d2,d3 = D[g+8][2t,2t+1]
-__device__ __forceinline__ void dmma16x8x4(double (&d)[4], double a0, double a1, double b0) {
-    asm volatile("mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, "
-                 "{%0,%1,%2,%3};\n"
-                 : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
-                 : "d"(a0), "d"(a1), "d"(b0));
-}
-
-// D = A(16x8, row) * B(8x8, col) + D.  Fragments: a0 = A[g][t], a1 = A[g+8][t],
+// D = A(16x8, row) * B(8x8, col) + D  (FP64 DMMA; g = lane/4, t = lane%4).  Fragments: a0 = A[g][t], a1 = A[g+8][t],
 //   a2 = A[g][t+4], a3 = A[g+8][t+4];  b0 = B[t][g], b1 = B[t+4][g];  D as for m16n8k4.
 __device__ __forceinline__ void dmma16x8x8(double (&d)[4], double a0, double a1, double a2,
                                            double a3, double b0, double b1) {
@@ -60,16 +52,15 @@ __device__ __forceinline__ void dmma16x8x8(double (&d)[4], double a0, double a1,
                  : "d"(a0), "d"(a1), "d"(a2), "d"(a3), "d"(b0), "d"(b1));
 }
 
-#ifndef CUEV_DMMA_K
-#define CUEV_DMMA_K 8 // k-depth of one DMMA instruction: 4 or 8
-#endif
-
 template <class C, bool TA, bool TB, bool SYMM> struct SmemLayout {
     // "outer-contiguous" tiles are stored [k][outer] (the global matrix is contiguous along the
     // outer index), the others [outer][k].
     static constexpr bool A_OUTER = SYMM || !TA;
     static constexpr bool B_OUTER = TB;
-    static constexpr int A_ELEMS = A_OUTER ? BK * (C::BM + PAD) : C::BM * (BK + PAD);
+    // SYMM stages hold either layout (tiles above the diagonal are read transposed)
+    static constexpr int A_ELEMS =
+        SYMM ? (BK * (C::BM + PAD) > C::BM * (BK + PAD) ? BK * (C::BM + PAD) : C::BM * (BK + PAD))
+             : (A_OUTER ? BK * (C::BM + PAD) : C::BM * (BK + PAD));
     static constexpr int B_ELEMS = B_OUTER ? BK * (C::BN + PAD) : C::BN * (BK + PAD);
     static constexpr int STAGE_ELEMS = A_ELEMS + B_ELEMS;
     static constexpr size_t BYTES = (size_t)C::STAGES * STAGE_ELEMS * sizeof(double);
@@ -113,10 +104,57 @@ __global__ void __launch_bounds__(C::NT)
     const int wm0 = (warp % C::WARPS_M) * C::WM;
     const int wn0 = (warp / C::WARPS_M) * C::WN;
 
+    // A tile of a SYMM stage: on/below the diagonal it is read as stored (m-contiguous, outer
+    // layout); above the diagonal its mirror A(kg, i) is read (k-contiguous, [m][k] layout).
+    auto symm_upper = [&](int k0) { return SYMM && (bm + C::BM - 1 < k0); };
     auto load_stage = [&](int slot, int k0) {
-        if (VEC == 2 && !SYMM) {
-            double *sA = smem + slot * L::STAGE_ELEMS;
-            double *sB = sA + L::A_ELEMS;
+        double *sA = smem + slot * L::STAGE_ELEMS;
+        double *sB = sA + L::A_ELEMS;
+        // ---- A tile: op(A)[bm .. bm+BM) x [k0 .. k0+BK)
+        if (SYMM) {
+            const bool upper = symm_upper(k0);
+            const bool lower = bm >= k0 + BK - 1;
+            if (VEC == 2 && (upper || lower)) {
+                if (lower) {
+#pragma unroll
+                    for (int it = 0; it < (C::BM / 2) * BK / C::NT; ++it) {
+                        const int e = tid + it * C::NT;
+                        const int r = 2 * (e % (C::BM / 2)), kk = e / (C::BM / 2);
+                        const int i = bm + r, kg = k0 + kk;
+                        const int nb = (i < m && kg < kend) ? (i + 1 < m ? 16 : 8) : 0;
+                        cp_async16(sA + kk * (C::BM + PAD) + r, nb ? A + i + (long long)kg * lda : A, nb);
+                    }
+                } else {
+#pragma unroll
+                    for (int it = 0; it < C::BM * (BK / 2) / C::NT; ++it) {
+                        const int e = tid + it * C::NT;
+                        const int kk = 2 * (e % (BK / 2)), r = e / (BK / 2);
+                        const int i = bm + r, kg = k0 + kk;
+                        const int nb = (i < m && kg < kend) ? (kg + 1 < kend ? 16 : 8) : 0;
+                        cp_async16(sA + r * (BK + PAD) + kk, nb ? A + kg + (long long)i * lda : A, nb);
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int it = 0; it < (C::BM * BK) / C::NT; ++it) {
+                    const int e = tid + it * C::NT;
+                    int r, kk;
+                    if (!upper) {
+                        r = e % C::BM;
+                        kk = e / C::BM;
+                    } else {
+                        kk = e % BK;
+                        r = e / BK;
+                    }
+                    const int i = bm + r, kg = k0 + kk;
+                    const bool pred = (i < m) && (kg < kend);
+                    const double *src = A;
+                    if (pred) src = (i >= kg) ? A + i + (long long)kg * lda : A + kg + (long long)i * lda;
+                    double *dst = upper ? sA + r * (BK + PAD) + kk : sA + kk * (C::BM + PAD) + r;
+                    cp_async8(dst, src, pred);
+                }
+            }
+        } else if (VEC == 2) {
             if (L::A_OUTER) { // A contiguous along m
 #pragma unroll
                 for (int it = 0; it < (C::BM / 2) * BK / C::NT; ++it) {
@@ -140,6 +178,35 @@ __global__ void __launch_bounds__(C::NT)
                     cp_async16(sA + r * (BK + PAD) + kk, src, nb);
                 }
             }
+        } else {
+#pragma unroll
+            for (int it = 0; it < (C::BM * BK) / C::NT; ++it) {
+                const int e = tid + it * C::NT;
+                int r, kk;
+                if (L::A_OUTER) {
+                    r = e % C::BM;
+                    kk = e / C::BM;
+                } else {
+                    kk = e % BK;
+                    r = e / BK;
+                }
+                const int i = bm + r, kg = k0 + kk;
+                const bool pred = (i < m) && (kg < kend);
+                const double *src = A;
+                if (pred) {
+                    if (kg < k1) {
+                        src = TA ? A + kg + (long long)i * lda : A + i + (long long)kg * lda;
+                    } else {
+                        const int q = kg - k1;
+                        src = TA ? A2 + q + (long long)i * lda2 : A2 + i + (long long)q * lda2;
+                    }
+                }
+                double *dst = L::A_OUTER ? sA + kk * (C::BM + PAD) + r : sA + r * (BK + PAD) + kk;
+                cp_async8(dst, src, pred);
+            }
+        }
+        // ---- B tile: op(B)[k0 .. k0+BK) x [bn .. bn+BN)
+        if (VEC == 2) {
             if (L::B_OUTER) { // B^T: contiguous along n
 #pragma unroll
                 for (int it = 0; it < (C::BN / 2) * BK / C::NT; ++it) {
@@ -163,64 +230,32 @@ __global__ void __launch_bounds__(C::NT)
                     cp_async16(sB + c * (BK + PAD) + kk, src, nb);
                 }
             }
-            return;
-        }
-        double *sA = smem + slot * L::STAGE_ELEMS;
-        double *sB = sA + L::A_ELEMS;
-        // ---- A tile: op(A)[bm .. bm+BM) x [k0 .. k0+BK)
-        const bool upper_tile = SYMM && (bm + C::BM - 1 < k0); // entirely above the diagonal
+        } else {
 #pragma unroll
-        for (int it = 0; it < (C::BM * BK) / C::NT; ++it) {
-            const int e = tid + it * C::NT;
-            int r, kk;
-            if (L::A_OUTER && !upper_tile) {
-                r = e % C::BM;
-                kk = e / C::BM;
-            } else {
-                kk = e % BK;
-                r = e / BK;
-            }
-            const int i = bm + r, kg = k0 + kk;
-            const bool pred = (i < m) && (kg < kend);
-            const double *src = A;
-            if (pred) {
-                if (SYMM) {
-                    src = (i >= kg) ? A + i + (long long)kg * lda : A + kg + (long long)i * lda;
-                } else if (kg < k1) {
-                    src = TA ? A + kg + (long long)i * lda : A + i + (long long)kg * lda;
+            for (int it = 0; it < (C::BN * BK) / C::NT; ++it) {
+                const int e = tid + it * C::NT;
+                int c, kk;
+                if (L::B_OUTER) {
+                    c = e % C::BN;
+                    kk = e / C::BN;
                 } else {
-                    const int q = kg - k1;
-                    src = TA ? A2 + q + (long long)i * lda2 : A2 + i + (long long)q * lda2;
+                    kk = e % BK;
+                    c = e / BK;
                 }
-            }
-            double *dst = L::A_OUTER ? sA + kk * (C::BM + PAD) + r : sA + r * (BK + PAD) + kk;
-            cp_async8(dst, src, pred);
-        }
-        // ---- B tile: op(B)[k0 .. k0+BK) x [bn .. bn+BN)
-#pragma unroll
-        for (int it = 0; it < (C::BN * BK) / C::NT; ++it) {
-            const int e = tid + it * C::NT;
-            int c, kk;
-            if (L::B_OUTER) {
-                c = e % C::BN;
-                kk = e / C::BN;
-            } else {
-                kk = e % BK;
-                c = e / BK;
-            }
-            const int j = bn + c, kg = k0 + kk;
-            const bool pred = (j < n) && (kg < kend);
-            const double *src = B;
-            if (pred) {
-                if (kg < k1) {
-                    src = TB ? B + j + (long long)kg * ldb : B + kg + (long long)j * ldb;
-                } else {
-                    const int q = kg - k1;
-                    src = TB ? B2 + j + (long long)q * ldb2 : B2 + q + (long long)j * ldb2;
+                const int j = bn + c, kg = k0 + kk;
+                const bool pred = (j < n) && (kg < kend);
+                const double *src = B;
+                if (pred) {
+                    if (kg < k1) {
+                        src = TB ? B + j + (long long)kg * ldb : B + kg + (long long)j * ldb;
+                    } else {
+                        const int q = kg - k1;
+                        src = TB ? B2 + j + (long long)q * ldb2 : B2 + q + (long long)j * ldb2;
+                    }
                 }
+                double *dst = L::B_OUTER ? sB + kk * (C::BN + PAD) + c : sB + c * (BK + PAD) + kk;
+                cp_async8(dst, src, pred);
             }
-            double *dst = L::B_OUTER ? sB + kk * (C::BN + PAD) + c : sB + c * (BK + PAD) + kk;
-            cp_async8(dst, src, pred);
         }
     };
 
@@ -232,24 +267,9 @@ __global__ void __launch_bounds__(C::NT)
 #pragma unroll
             for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.0;
 
-    // prologue
-#pragma unroll
-    for (int s = 0; s < C::STAGES - 1; ++s) {
-        if (s < ntiles) load_stage(s, kbeg + s * BK);
-        cp_async_commit();
-    }
-
-    for (int kt = 0; kt < ntiles; ++kt) {
-        cp_async_wait<C::STAGES - 2>();
-        __syncthreads();
-        {
-            const int pf = kt + C::STAGES - 1;
-            if (pf < ntiles) load_stage(pf % C::STAGES, kbeg + pf * BK);
-            cp_async_commit();
-        }
-        const double *sA = smem + (kt % C::STAGES) * L::STAGE_ELEMS;
-        const double *sB = sA + L::A_ELEMS;
-#if CUEV_DMMA_K == 8
+    // one BK-deep stage of DMMA work; AOUT selects the A tile layout of this stage
+    auto mma_stage = [&](const double *sA, const double *sB, auto aout) {
+        constexpr bool AOUT = decltype(aout)::value;
 #pragma unroll
         for (int ks = 0; ks < BK / 8; ++ks) {
             const int kk = ks * 8 + t;
@@ -260,7 +280,7 @@ __global__ void __launch_bounds__(C::NT)
 #pragma unroll
                 for (int hh = 0; hh < 2; ++hh) { // k offset 0 / 4
                     const int k2 = kk + 4 * hh;
-                    if (L::A_OUTER) {
+                    if (AOUT) {
                         af[mi][2 * hh] = sA[k2 * (C::BM + PAD) + r];
                         af[mi][2 * hh + 1] = sA[k2 * (C::BM + PAD) + r + 8];
                     } else {
@@ -285,34 +305,29 @@ __global__ void __launch_bounds__(C::NT)
                     dmma16x8x8(acc[mi][ni], af[mi][0], af[mi][1], af[mi][2], af[mi][3], bf[ni][0],
                                bf[ni][1]);
         }
-#else
+    };
+
+    // prologue
 #pragma unroll
-        for (int ks = 0; ks < BK / 4; ++ks) {
-            const int kk = ks * 4 + t;
-            double af[C::MT][2], bf[C::NTL];
-#pragma unroll
-            for (int mi = 0; mi < C::MT; ++mi) {
-                const int r = wm0 + mi * 16 + g;
-                if (L::A_OUTER) {
-                    af[mi][0] = sA[kk * (C::BM + PAD) + r];
-                    af[mi][1] = sA[kk * (C::BM + PAD) + r + 8];
-                } else {
-                    af[mi][0] = sA[r * (BK + PAD) + kk];
-                    af[mi][1] = sA[(r + 8) * (BK + PAD) + kk];
-                }
-            }
-#pragma unroll
-            for (int ni = 0; ni < C::NTL; ++ni) {
-                const int c = wn0 + ni * 8 + g;
-                bf[ni] = L::B_OUTER ? sB[kk * (C::BN + PAD) + c] : sB[c * (BK + PAD) + kk];
-            }
-#pragma unroll
-            for (int mi = 0; mi < C::MT; ++mi)
-#pragma unroll
-                for (int ni = 0; ni < C::NTL; ++ni)
-                    dmma16x8x4(acc[mi][ni], af[mi][0], af[mi][1], bf[ni]);
+    for (int s = 0; s < C::STAGES - 1; ++s) {
+        if (s < ntiles) load_stage(s, kbeg + s * BK);
+        cp_async_commit();
+    }
+
+    for (int kt = 0; kt < ntiles; ++kt) {
+        cp_async_wait<C::STAGES - 2>();
+        __syncthreads();
+        {
+            const int pf = kt + C::STAGES - 1;
+            if (pf < ntiles) load_stage(pf % C::STAGES, kbeg + pf * BK);
+            cp_async_commit();
         }
-#endif
+        const double *sA = smem + (kt % C::STAGES) * L::STAGE_ELEMS;
+        const double *sB = sA + L::A_ELEMS;
+        if (SYMM && symm_upper(kbeg + kt * BK))
+            mma_stage(sA, sB, std::integral_constant<bool, false>{});
+        else
+            mma_stage(sA, sB, std::integral_constant<bool, L::A_OUTER>{});
     }
     cp_async_wait<0>();
 
@@ -383,7 +398,10 @@ int launch_cfg(const GemmArgs &a, const GemmArgs *dev_args, dim3 grid, cudaStrea
 template <class C, bool SYMM, bool BATCHED>
 int dispatch_t(const GemmArgs &a, const GemmArgs *dev_args, int ta, int tb, dim3 grid,
                cudaStream_t stream, bool vec2 = false) {
-    if (SYMM) return launch_cfg<C, false, false, true, BATCHED, 1>(a, dev_args, grid, stream);
+    if (SYMM) {
+        if (vec2) return launch_cfg<C, false, false, true, BATCHED, 2>(a, dev_args, grid, stream);
+        return launch_cfg<C, false, false, true, BATCHED, 1>(a, dev_args, grid, stream);
+    }
     if (BATCHED) return launch_cfg<C, false, false, false, BATCHED, 1>(a, dev_args, grid, stream);
     if (vec2) {
         if (!ta && !tb) return launch_cfg<C, false, false, false, false, 2>(a, dev_args, grid, stream);
@@ -402,7 +420,7 @@ bool aligned16(const void *p) { return ((uintptr_t)p & 15) == 0; }
 // 16-byte loads are legal when every base is 16-byte aligned, every leading dimension is even
 // (so each column starts 16-byte aligned) and the first K segment has even length.
 bool vec2_ok(const GemmArgs &a) {
-    if (a.symm_a) return false;
+    if (a.symm_a) return aligned16(a.A) && aligned16(a.B) && !(a.lda & 1) && !(a.ldb & 1);
     if (!aligned16(a.A) || !aligned16(a.B) || (a.lda & 1) || (a.ldb & 1)) return false;
     if (a.k2 > 0 && (!aligned16(a.A2) || !aligned16(a.B2) || (a.lda2 & 1) || (a.ldb2 & 1) || (a.k & 1)))
         return false;
@@ -470,19 +488,19 @@ int gemm_launch(const GemmArgs &a_in, int ta, int tb, cudaStream_t stream) {
     int st;
     switch (tl) {
     case Tile::Big:
-        st = a.symm_a ? dispatch_t<CfgBig, true, false>(a, nullptr, 0, 0, grid, stream)
+        st = a.symm_a ? dispatch_t<CfgBig, true, false>(a, nullptr, 0, 0, grid, stream, v2)
                       : dispatch_t<CfgBig, false, false>(a, nullptr, ta, tb, grid, stream, v2);
         break;
     case Tile::Skinny:
-        st = a.symm_a ? dispatch_t<CfgSkinny, true, false>(a, nullptr, 0, 0, grid, stream)
+        st = a.symm_a ? dispatch_t<CfgSkinny, true, false>(a, nullptr, 0, 0, grid, stream, v2)
                       : dispatch_t<CfgSkinny, false, false>(a, nullptr, ta, tb, grid, stream, v2);
         break;
     case Tile::N32:
-        st = a.symm_a ? dispatch_t<CfgN32, true, false>(a, nullptr, 0, 0, grid, stream)
+        st = a.symm_a ? dispatch_t<CfgN32, true, false>(a, nullptr, 0, 0, grid, stream, v2)
                       : dispatch_t<CfgN32, false, false>(a, nullptr, ta, tb, grid, stream, v2);
         break;
     default:
-        st = a.symm_a ? dispatch_t<CfgSmall, true, false>(a, nullptr, 0, 0, grid, stream)
+        st = a.symm_a ? dispatch_t<CfgSmall, true, false>(a, nullptr, 0, 0, grid, stream, v2)
                       : dispatch_t<CfgSmall, false, false>(a, nullptr, ta, tb, grid, stream, v2);
         break;
     }

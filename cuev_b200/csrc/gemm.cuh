@@ -1,7 +1,7 @@
 // FP64 tensor-core GEMM for sm_100a: C = alpha * op(A) * op(B) + beta * C, column-major.
 //
 // tcgen05 has no f64 kind, so FP64 contractions run on the DMMA path
-// (`mma.sync.aligned.m16n8k4.row.col.f64`), fed by a multi-stage cp.async shared-memory
+// (`mma.sync.aligned.m16n8k8.row.col.f64`), fed by a multi-stage cp.async shared-memory
 // pipeline.  One kernel template covers every contraction the solver needs:
 //   - plain GEMM with op(A), op(B) in {N, T}                       (reference cublas::gemm)
 //   - SYMM with A symmetric, lower triangle read                  (reference cublas::symm LOWER)
