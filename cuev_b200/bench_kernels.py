@@ -1,0 +1,150 @@
+"""Per-kernel timings of libcuev_b200 through its C ABI (CUDA events on the launching stream).
+
+    python -m cuev_b200.bench_kernels gemm M N K [--ta] [--tb]   DMMA GEMM vs torch (cuBLAS)
+    python -m cuev_b200.bench_kernels symm M N                   C = A B, A symmetric (lower)
+    python -m cuev_b200.bench_kernels syr2k N K                  lower(C) = A B^T + B A^T
+    python -m cuev_b200.bench_kernels stages N                   every solver stage on its own
+
+`stages` runs the pipeline through the stage entry points (cuev_dbbr_reduce, cuev_bc_chase,
+cuev_tridi_dc, cuev_bc_back, cuev_sbr_back) with an event pair around each, so a profiler can
+select one stage's kernels with few launches before them.  Inputs are seeded random matrices
+(A = (G + G^T)/2, G iid N(0,1)).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import statistics
+
+import torch
+
+import cuev_b200 as cv
+
+
+def _time(fn, reps: int, warmup: int) -> float:
+    """Median milliseconds of fn() over reps launches, after warmup launches."""
+    st = torch.cuda.current_stream()
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    out = []
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        fn()
+        e1.record(st)
+        torch.cuda.synchronize()
+        out.append(e0.elapsed_time(e1))
+    return statistics.median(out)
+
+
+def _rand(rows, cols, seed):
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    return torch.randn(rows, cols, dtype=torch.float64, device="cuda", generator=g)
+
+
+def run_gemm(a):
+    m, n, k = a.M, a.N, a.K
+    # column-major operands: a (rows x cols) column-major matrix is a (cols, rows) torch tensor
+    A = _rand(m if a.ta else k, k if a.ta else m, 1)   # op(A) = m x k
+    B = _rand(k if a.tb else n, n if a.tb else k, 2)   # op(B) = k x n
+    Cm = torch.zeros(n, m, dtype=torch.float64, device="cuda")
+    lda = k if a.ta else m
+    ldb = n if a.tb else k
+    ms = _time(lambda: cv.dgemm(a.ta, a.tb, m, n, k, 1.0, A, lda, B, ldb, 0.0, Cm, m),
+               a.reps, a.warmup)
+    # cuBLAS on the same product, for scale
+    At = A.t() if not a.ta else A       # logical op(A) as a row-major (m, k) view
+    Bt = B.t() if not a.tb else B
+    ref_ms = _time(lambda: torch.matmul(At, Bt), a.reps, a.warmup)
+    fl = 2.0 * m * n * k
+    return {"kernel": "dgemm", "m": m, "n": n, "k": k, "ta": a.ta, "tb": a.tb,
+            "ms": round(ms, 4), "tflops": round(fl / ms / 1e9, 3),
+            "cublas_ms": round(ref_ms, 4), "cublas_tflops": round(fl / ref_ms / 1e9, 3)}
+
+
+def run_symm(a):
+    m, n = a.M, a.N
+    A = _rand(m, m, 1)
+    B = _rand(n, m, 2)
+    Cm = torch.zeros(n, m, dtype=torch.float64, device="cuda")
+    ms = _time(lambda: cv.dsymm_lower(m, n, 1.0, A, m, B, m, 0.0, Cm, m), a.reps, a.warmup)
+    fl = 2.0 * m * m * n
+    return {"kernel": "dsymm_lower", "m": m, "n": n, "ms": round(ms, 4),
+            "tflops": round(fl / ms / 1e9, 3)}
+
+
+def run_syr2k(a):
+    n, k = a.M, a.N
+    A = _rand(k, n, 1)
+    B = _rand(k, n, 2)
+    Cm = torch.zeros(n, n, dtype=torch.float64, device="cuda")
+    ms = _time(lambda: cv.dsyr2k_lower(n, k, 1.0, A, n, B, n, 0.0, Cm, n), a.reps, a.warmup)
+    fl = 2.0 * n * n * k  # lower triangle of two products
+    return {"kernel": "dsyr2k_lower", "n": n, "k": k, "ms": round(ms, 4),
+            "tflops": round(fl / ms / 1e9, 3)}
+
+
+def run_stages(a):
+    n = a.M
+    A0 = _rand(n, n, 7)
+    A0 = ((A0 + A0.t()) * 0.5).contiguous()
+    A = torch.empty_like(A0)
+    h = cv.SolverHandle(n, a.nbw, a.nk)
+    try:
+        b = a.nbw
+        Bt, ldb = h.buffer(cv.BUF_B, 2 * b, n)
+        d = torch.empty(n, dtype=torch.float64, device="cuda")
+        e = torch.empty(n, dtype=torch.float64, device="cuda")
+        w = torch.empty(n, dtype=torch.float64, device="cuda")
+        V = torch.empty(n, n, dtype=torch.float64, device="cuda")
+        names = ["dbbr_reduce", "bc_chase", "tridi_dc", "bc_back", "sbr_back"]
+        times = {k: [] for k in names}
+        st = torch.cuda.current_stream()
+        for rep in range(a.warmup + a.reps):
+            A.copy_(A0)
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(len(names) + 1)]
+            ev[0].record(st)
+            h.dbbr_reduce(A)
+            ev[1].record(st)
+            h.bc_chase(Bt, d, e)
+            ev[2].record(st)
+            h.tridi_dc(d, e, w, V)
+            ev[3].record(st)
+            h.bc_back(V, n)
+            ev[4].record(st)
+            h.sbr_back(V, n)
+            ev[5].record(st)
+            torch.cuda.synchronize()
+            if rep >= a.warmup:
+                for i, k in enumerate(names):
+                    times[k].append(ev[i].elapsed_time(ev[i + 1]))
+        out = {k: round(statistics.median(v), 3) for k, v in times.items()} if a.reps else {}
+        flops = {"bc_back": 2.0 * n ** 3, "sbr_back": 2.0 * n ** 3}
+        rates = {k + "_tflops": round(flops[k] / out[k] / 1e9, 3) for k in flops if k in out}
+        return {"kernel": "stages", "n": n, "nbw": a.nbw, "nk": a.nk, "ms": out, **rates}
+    finally:
+        h.close()
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("what", choices=["gemm", "symm", "syr2k", "stages"])
+    ap.add_argument("M", type=int)
+    ap.add_argument("N", type=int, nargs="?", default=0)
+    ap.add_argument("K", type=int, nargs="?", default=0)
+    ap.add_argument("--ta", type=int, default=0)
+    ap.add_argument("--tb", type=int, default=0)
+    ap.add_argument("--nbw", type=int, default=32)
+    ap.add_argument("--nk", type=int, default=0)
+    ap.add_argument("--reps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=2)
+    a = ap.parse_args(argv)
+    if a.what == "stages" and a.nk == 0:
+        a.nk = 512 if a.M >= 8192 else 256
+    fn = {"gemm": run_gemm, "symm": run_symm, "syr2k": run_syr2k, "stages": run_stages}[a.what]
+    print(json.dumps(fn(a)), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -195,13 +195,286 @@ template <int BW, int TS> int launch_bc_back(Workspace *ws, double *M, long long
     return CUEV_OK;
 }
 
+
+// ---------------------------------------------------------------------------------------------
+// Pipelined BC-Back for b = 32.
+//
+// The one-thread-per-column kernel above has only n threads of parallelism (n/32 warps: about
+// 3.5 warps per SM at n = 16384), far too few to hide FP64 and shared-memory latency.  Here a
+// CTA owns 32 columns and runs P warps over P consecutive sweep tiles at once, as a pipeline:
+// warp p applies tile t while warp p+1 applies tile t-1 one hop block behind it.  Tile t emits
+// its finished rows in hop order, chunk h = rows [top_t + 32h, top_t + 32h + 32); with a window
+// of TS + 32 rows (KEEP = TS), the rows tile t-1 takes in at hop h are exactly chunk h of tile t,
+// and the rows [top_{t-1}, top_t) it starts with have never been touched by a later tile, so they
+// come straight from M.  Rows move between the warps of one round through shared-memory rings of
+// two chunks (row-major [32 rows][32 columns]: lane c reads and writes column c, conflict-free);
+// the last warp of a round hands its rows to the first warp of the next round through a global
+// buffer X in the same row-major layout (256-byte coalesced rows), and only the warp that applies
+// tile 0 writes M.  Each row of M is thus read once and written once; X is written and read once
+// per round of P tiles.  Every wait is on a shared-memory counter, bounded by time, and all the
+// warps that wait on one another belong to one CTA (so they are co-resident).
+//
+// Per hop a warp applies TS reflectors of length 32 to its 32 columns: the reflector is loaded
+// once from shared memory (16 broadcast 16-byte loads) into registers and used for both the dot
+// product and the update, 64 FMAs per lane per reflector.
+constexpr int PB = 32;
+
+template <int TS, int P> struct PipeSmem {
+    double w[P][2][TS][PB];        // reflectors of each warp's current and next hop block
+    double ring[P - 1][2][PB][32]; // warp p -> warp p+1, two chunks of 32 rows x 32 columns
+    double xin[2][PB][32];         // warp 0: incoming rows (from X or, first tile, from M)
+    int prod[P], cons[P];          // ring p: chunks written / chunks fully read (monotonic)
+    int gprog;                     // chunks the last warp has written to X (monotonic)
+    int abort_flag;                // set by a warp that gave up waiting
+};
+
+__device__ __forceinline__ int lds_acquire(const int *p) {
+    int v;
+    asm volatile("ld.acquire.cta.shared::cta.b32 %0, [%1];"
+                 : "=r"(v)
+                 : "r"((unsigned)__cvta_generic_to_shared(p))
+                 : "memory");
+    return v;
+}
+__device__ __forceinline__ void sts_release(int *p, int v) {
+    asm volatile("st.release.cta.shared::cta.b32 [%0], %1;" ::"r"(
+                     (unsigned)__cvta_generic_to_shared(p)),
+                 "r"(v)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async16_cg(void *smem, const void *gmem, bool pred) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gmem),
+                 "r"(pred ? 16 : 0)
+                 : "memory");
+}
+
+// Wait (all lanes) until *flag >= target.  Gives up after 2 s or when another warp gave up;
+// returns false then (the caller returns after draining its copies).
+__device__ __forceinline__ bool pipe_wait(const int *flag, int target, int *abort_flag,
+                                          int *status, int where) {
+    if (lds_acquire(flag) >= target) return true;
+    const uint64_t t0 = global_ns();
+    for (;;) {
+        __nanosleep(32);
+        if (lds_acquire(flag) >= target) return true;
+        if (*(volatile int *)abort_flag) return false;
+        if (global_ns() - t0 > 2000000000ull) {
+            dev_fail(status, CUEV_ERR_TIMEOUT, where);
+            *(volatile int *)abort_flag = 1;
+            return false;
+        }
+    }
+}
+
+template <int TS, int P>
+__global__ void __launch_bounds__(32 * P, 1)
+    bc_back_pipe_kernel(const double *__restrict__ U, long long ldu, double *__restrict__ M,
+                        long long ldm, double *__restrict__ X, int n, int ncols,
+                        int *__restrict__ status) {
+    constexpr int R = TS + PB; // register window rows
+    extern __shared__ __align__(16) unsigned char pipe_smem_raw[];
+    PipeSmem<TS, P> &S = *reinterpret_cast<PipeSmem<TS, P> *>(pipe_smem_raw);
+    const int lane = threadIdx.x & 31, p = threadIdx.x >> 5;
+    const int col0 = blockIdx.x * 32;
+    const int mycol = min(col0 + lane, ncols - 1); // clamped: lanes past ncols never store to M
+    const bool active = col0 + lane < ncols;
+    const double *Mc = M + (long long)mycol * ldm;
+    double *Xg = X + (size_t)blockIdx.x * n * 32; // row r of this CTA's columns: Xg[32 r + lane]
+    const int nsweeps = n - 2;
+    const int T = (nsweeps + TS - 1) / TS;
+    if (threadIdx.x < P) S.prod[threadIdx.x] = 0, S.cons[threadIdx.x] = 0;
+    if (threadIdx.x == 0) S.gprog = 0, S.abort_flag = 0;
+    __syncthreads(); // the only CTA-wide barrier: warps leave at different times
+
+    // reflectors (s0 + j, hop of `rbase`): rows [rbase + j, rbase + j + 32) of U[:, s0 + j]
+    auto stage_w = [&](int buf, int s0, int rbase) {
+#pragma unroll
+        for (int j = 0; j < TS; ++j) {
+            const int s = s0 + j, row = rbase + j + lane;
+            const bool ok = (s < nsweeps) && (row < n);
+            cp_async8(&S.w[p][buf][j][lane], ok ? U + row + (long long)s * ldu : U, ok);
+        }
+    };
+    // warp 0's incoming chunk: 32 rows from X (coalesced 16-byte copies) ...
+    auto stage_x = [&](int buf, int row0) {
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+            const int e = q * 64 + lane * 2; // element pair (row e / 32, columns e % 32, +1)
+            const int r = row0 + (e >> 5);
+            const bool ok = r < n;
+            cp_async16_cg(&S.xin[buf][e >> 5][e & 31], ok ? Xg + (size_t)r * 32 + (e & 31) : Xg,
+                          ok);
+        }
+    };
+    // ... or, for the first tile, from M (one column per lane)
+    auto stage_m = [&](int buf, int row0) {
+#pragma unroll
+        for (int i = 0; i < PB; ++i) {
+            const int r = row0 + i;
+            const bool ok = r < n;
+            cp_async8(&S.xin[buf][i][lane], ok ? Mc + r : Mc, ok);
+        }
+    };
+
+    double m[R];
+    int oseq = 0;  // chunks this warp has put into ring p (or X, for the last warp)
+    int iseq = 0;  // chunks this warp has taken from ring p-1
+    int xbase = 0; // warp 0: X sequence number of the current input tile's chunk 0
+    bool ok = true;
+    for (int t = T - 1 - p; t >= 0 && ok; t -= P) {
+        const int s0 = t * TS;
+        const int top = s0 + 1;
+        const int hmax = (n - 1 - top) / PB;
+        const bool has_in = t + 1 <= T - 1; // rows [top + TS, n) come from tile t + 1
+        const int top_in = top + TS;
+        const int hmax_in = has_in ? (n - 1 - top_in) / PB : -1;
+        const bool first = !has_in; // only warp 0 of the first round
+        const bool to_m = t == 0;
+        const bool to_x = !to_m && p == P - 1;
+
+        __syncwarp();
+        stage_w(0, s0, top);
+        if (p == 0) {
+            if (first) {
+                stage_m(0, top_in);
+            } else if (hmax_in >= 0) {
+                if (!pipe_wait(&S.gprog, xbase + 1, &S.abort_flag, status, -1)) { ok = false; break; }
+                stage_x(0, top_in);
+            }
+        }
+        cp_async_commit();
+#pragma unroll
+        for (int i = 0; i < TS; ++i) {
+            const int row = top + i;
+            const double v = Mc[min(row, n - 1)];
+            m[i] = row < n ? v : 0.0;
+        }
+        for (int h = 0; h <= hmax; ++h) {
+            const int base = top + h * PB; // row of m[0]
+            cp_async_wait<0>();
+            __syncwarp();
+            if (h < hmax) {
+                stage_w((h + 1) & 1, s0, base + PB);
+                if (p == 0) {
+                    if (first) {
+                        stage_m((h + 1) & 1, top_in + (h + 1) * PB);
+                    } else if (h + 1 <= hmax_in) {
+                        if (!pipe_wait(&S.gprog, xbase + h + 2, &S.abort_flag, status, -2)) {
+                            ok = false;
+                            break;
+                        }
+                        stage_x((h + 1) & 1, top_in + (h + 1) * PB);
+                    }
+                }
+            }
+            cp_async_commit();
+
+            // incoming rows m[TS .. TS+32) = rows [base + TS, base + TS + 32) = chunk h of tile t+1
+            if (p == 0) {
+                if (first || h <= hmax_in) {
+#pragma unroll
+                    for (int i = 0; i < PB; ++i) m[TS + i] = S.xin[h & 1][i][lane];
+                } else {
+#pragma unroll
+                    for (int i = 0; i < PB; ++i) m[TS + i] = 0.0;
+                }
+            } else if (h <= hmax_in) {
+                if (!pipe_wait(&S.prod[p - 1], iseq + 1, &S.abort_flag, status, -3)) {
+                    ok = false;
+                    break;
+                }
+                const int slot = iseq & 1;
+#pragma unroll
+                for (int i = 0; i < PB; ++i) m[TS + i] = S.ring[p - 1][slot][i][lane];
+                __syncwarp();
+                ++iseq;
+                if (lane == 0) sts_release(&S.cons[p - 1], iseq);
+            } else {
+#pragma unroll
+                for (int i = 0; i < PB; ++i) m[TS + i] = 0.0;
+            }
+
+            // apply the tile's reflectors of this hop, last sweep first
+            const double *W = &S.w[p][h & 1][0][0];
+#pragma unroll
+            for (int j = TS - 1; j >= 0; --j) {
+                double wr[PB];
+#pragma unroll
+                for (int i = 0; i < PB; i += 2) {
+                    const double2 v = lds2(W + j * PB + i);
+                    wr[i] = v.x, wr[i + 1] = v.y;
+                }
+                double acc[8];
+#pragma unroll
+                for (int i = 0; i < 8; ++i) acc[i] = wr[i] * m[j + i];
+#pragma unroll
+                for (int i = 8; i < PB; ++i) acc[i & 7] = fma(wr[i], m[j + i], acc[i & 7]);
+                const double f = -2.0 * (((acc[0] + acc[1]) + (acc[2] + acc[3])) +
+                                         ((acc[4] + acc[5]) + (acc[6] + acc[7])));
+#pragma unroll
+                for (int i = 0; i < PB; ++i) m[j + i] = fma(f, wr[i], m[j + i]);
+            }
+
+            // rows [base, base + 32) are final for this tile
+            if (to_m) {
+                if (active) {
+                    double *Mw = M + (long long)mycol * ldm;
+#pragma unroll
+                    for (int i = 0; i < PB; ++i)
+                        if (base + i < n) Mw[base + i] = m[i];
+                }
+            } else if (to_x) {
+#pragma unroll
+                for (int i = 0; i < PB; ++i)
+                    if (base + i < n) __stcg(Xg + (size_t)(base + i) * 32 + lane, m[i]);
+                __threadfence();
+                __syncwarp();
+                ++oseq;
+                if (lane == 0) sts_release(&S.gprog, oseq);
+            } else {
+                if (!pipe_wait(&S.cons[p], oseq - 1, &S.abort_flag, status, -4)) {
+                    ok = false;
+                    break;
+                }
+                const int slot = oseq & 1;
+#pragma unroll
+                for (int i = 0; i < PB; ++i) S.ring[p][slot][i][lane] = m[i];
+                __syncwarp();
+                ++oseq;
+                if (lane == 0) sts_release(&S.prod[p], oseq);
+            }
+#pragma unroll
+            for (int i = 0; i < TS; ++i) m[i] = m[i + PB];
+        }
+        if (p == 0 && has_in) xbase += hmax_in + 1;
+    }
+    cp_async_wait<0>(); // leave no copy in flight, also on the early exits
+}
+
+template <int TS, int P> int launch_bc_back_pipe(Workspace *ws, double *M, long long ldm) {
+    const int n = ws->n;
+    const size_t smem = sizeof(PipeSmem<TS, P>);
+    auto kern = bc_back_pipe_kernel<TS, P>;
+    static bool attr = false;
+    if (!attr) {
+        CUEV_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr = true;
+    }
+    const int grid = div_up(n, 32);
+    kern<<<grid, 32 * P, smem, ws->stream>>>(ws->U, ws->n, M, ldm, ws->dc_S, n, n, ws->status);
+    note_launch();
+    CUEV_TRY(cudaGetLastError());
+    return CUEV_OK;
+}
+
 } // namespace
 
 int bc_back(Workspace *ws, double *M, long long ldm) {
     if (ws->n <= 2) return CUEV_OK;
     // register window R = TS + b - 1 rows: 79 rows keeps b = 32 spill-free (252 registers);
     // b = 64 needs the 64 reflector entries live as well and runs a shorter tile
-    if (ws->b == 32) return launch_bc_back<32, 48>(ws, M, ldm, ws->n);
+    if (ws->b == 32) return launch_bc_back_pipe<16, 8>(ws, M, ldm);
     if (ws->b == 64) return launch_bc_back<64, 16>(ws, M, ldm, ws->n);
     return CUEV_ERR_INVALID;
 }

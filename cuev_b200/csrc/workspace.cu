@@ -39,7 +39,8 @@ int workspace_create(int n, int b, int k, cudaStream_t stream, Workspace **out) 
         {(void **)&ws->Y, nn * s},
         {(void **)&ws->U, nn * s},
         {(void **)&ws->dc_Q2, nn * s},
-        {(void **)&ws->dc_S, nn * s},
+        // dc_S also carries BC-Back's round-to-round rows: ceil(n/32) groups of n x 32
+        {(void **)&ws->dc_S, N * ((N + 31) / 32 * 32) * s},
         {(void **)&ws->dc_T, nn * s},
         {(void **)&ws->Z, N * k * s},
         {(void **)&ws->Wp, N * b * s},
