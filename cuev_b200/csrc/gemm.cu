@@ -10,16 +10,18 @@ namespace {
 constexpr int BK = 16; // k-depth of one shared-memory stage (4 DMMA k-steps)
 constexpr int PAD = 4; // row padding (doubles): keeps fragment reads bank-conflict free
 
-template <int BM_, int BN_, int WARPS_M_, int WARPS_N_, int STAGES_> struct TileCfg {
+// KS_: k-depth of one DMMA (8 or 16); the k16 shape needs twice the fragment registers.
+template <int BM_, int BN_, int WARPS_M_, int WARPS_N_, int STAGES_, int KS_ = 16> struct TileCfg {
     static constexpr int BM = BM_, BN = BN_, WARPS_M = WARPS_M_, WARPS_N = WARPS_N_;
-    static constexpr int STAGES = STAGES_;
+    static constexpr int STAGES = STAGES_, KS = KS_;
+    static_assert(KS == 8 || KS == 16, "DMMA k-depth");
     static constexpr int NT = 32 * WARPS_M * WARPS_N;
     static constexpr int WM = BM / WARPS_M, WN = BN / WARPS_N;
     static constexpr int MT = WM / 16, NTL = WN / 8;
     static_assert(WM % 16 == 0 && WN % 8 == 0, "warp tile must be a multiple of the DMMA shape");
 };
 
-using CfgBig = TileCfg<128, 128, 2, 4, 3>;
+using CfgBig = TileCfg<128, 128, 4, 4, 4, 8>; // 16 warps: two per SMSP left the DMMA pipe idle
 using CfgSkinny = TileCfg<128, 64, 4, 2, 4>;
 using CfgSmall = TileCfg<64, 64, 2, 2, 4>;
 using CfgN32 = TileCfg<256, 32, 8, 1, 4>; // N <= 32 (band width 32 panels)
@@ -50,6 +52,17 @@ __device__ __forceinline__ void dmma16x8x8(double (&d)[4], double a0, double a1,
                  "{%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
                  : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
                  : "d"(a0), "d"(a1), "d"(a2), "d"(a3), "d"(b0), "d"(b1));
+}
+
+// D = A(16x16, row) * B(16x8, col) + D (FP64 DMMA, sm_90+ shape).  Fragments extend the k8 layout:
+//   a[2i] = A[g][t + 4i], a[2i+1] = A[g+8][t + 4i];  b[i] = B[t + 4i][g]  (i = 0..3).
+__device__ __forceinline__ void dmma16x8x16(double (&d)[4], const double (&a)[8],
+                                            const double (&b)[4]) {
+    asm volatile("mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, "
+                 "{%4,%5,%6,%7,%8,%9,%10,%11}, {%12,%13,%14,%15}, {%0,%1,%2,%3};\n"
+                 : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+                 : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]),
+                   "d"(a[7]), "d"(b[0]), "d"(b[1]), "d"(b[2]), "d"(b[3]));
 }
 
 template <class C, bool TA, bool TB, bool SYMM> struct SmemLayout {
@@ -270,15 +283,16 @@ __global__ void __launch_bounds__(C::NT)
     // one BK-deep stage of DMMA work; AOUT selects the A tile layout of this stage
     auto mma_stage = [&](const double *sA, const double *sB, auto aout) {
         constexpr bool AOUT = decltype(aout)::value;
+        constexpr int KS = C::KS, NH = KS / 4; // fragment entries per row: k offsets 0, 4, ...
 #pragma unroll
-        for (int ks = 0; ks < BK / 8; ++ks) {
-            const int kk = ks * 8 + t;
-            double af[C::MT][4], bf[C::NTL][2];
+        for (int ks = 0; ks < BK / KS; ++ks) {
+            const int kk = ks * KS + t;
+            double af[C::MT][2 * NH], bf[C::NTL][NH];
 #pragma unroll
             for (int mi = 0; mi < C::MT; ++mi) {
                 const int r = wm0 + mi * 16 + g;
 #pragma unroll
-                for (int hh = 0; hh < 2; ++hh) { // k offset 0 / 4
+                for (int hh = 0; hh < NH; ++hh) {
                     const int k2 = kk + 4 * hh;
                     if (AOUT) {
                         af[mi][2 * hh] = sA[k2 * (C::BM + PAD) + r];
@@ -293,7 +307,7 @@ __global__ void __launch_bounds__(C::NT)
             for (int ni = 0; ni < C::NTL; ++ni) {
                 const int c = wn0 + ni * 8 + g;
 #pragma unroll
-                for (int hh = 0; hh < 2; ++hh) {
+                for (int hh = 0; hh < NH; ++hh) {
                     const int k2 = kk + 4 * hh;
                     bf[ni][hh] = L::B_OUTER ? sB[k2 * (C::BN + PAD) + c] : sB[c * (BK + PAD) + k2];
                 }
@@ -301,9 +315,13 @@ __global__ void __launch_bounds__(C::NT)
 #pragma unroll
             for (int mi = 0; mi < C::MT; ++mi)
 #pragma unroll
-                for (int ni = 0; ni < C::NTL; ++ni)
-                    dmma16x8x8(acc[mi][ni], af[mi][0], af[mi][1], af[mi][2], af[mi][3], bf[ni][0],
-                               bf[ni][1]);
+                for (int ni = 0; ni < C::NTL; ++ni) {
+                    if constexpr (KS == 16)
+                        dmma16x8x16(acc[mi][ni], af[mi], bf[ni]);
+                    else
+                        dmma16x8x8(acc[mi][ni], af[mi][0], af[mi][1], af[mi][2], af[mi][3],
+                                   bf[ni][0], bf[ni][1]);
+                }
         }
     };
 
