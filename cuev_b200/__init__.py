@@ -56,8 +56,10 @@ class Config(C.Structure):
 
 
 class RefineInfo(C.Structure):
-    _fields_ = [("iters", C.c_int), ("resid", C.c_double), ("orth", C.c_double),
-                ("stage1_ms", C.c_float), ("refine_ms", C.c_float)]
+    """cuev_refine_info: steps applied and the norms measured on the last X."""
+
+    _fields_ = [("iterations", C.c_int), ("offdiag_fro", C.c_double), ("orth_fro", C.c_double),
+                ("anorm", C.c_double)]
 
 
 _VP, _I, _D, _DP, _FP = C.c_void_p, C.c_int, C.c_double, C.c_void_p, C.c_void_p
@@ -81,7 +83,7 @@ _SIGS = {
     "cuev_dgemm_noalloc": [_VP, _I, _I, _I, _I, _I, _D, _DP, _I, _DP, _I, _D, _DP, _I],
     "cuev_dsymm_lower": [_VP, _I, _I, _D, _DP, _I, _DP, _I, _D, _DP, _I],
     "cuev_dsyr2k_lower": [_VP, _I, _I, _D, _DP, _I, _DP, _I, _D, _DP, _I],
-    "cuev_dsyevd_mixed": [_DP, _I, _DP, _DP, _I, _D, _VP, C.POINTER(RefineInfo)],
+    "cuev_dsyev_refine": [_DP, _I, _DP, _DP, _I, _D, _VP, C.POINTER(RefineInfo)],
     "cuev_dsyev_adjoint": [_DP, _DP, _DP, _DP, _I, _D, _DP, _VP],
     "cuev_ssyev_adjoint": [_FP, _FP, _FP, _FP, _I, C.c_float, _FP, _VP],
 }
@@ -179,6 +181,19 @@ def eigh(A_rowmajor_sym, nbw: int = 0, nk: int = 0):
     Vcm = torch.empty_like(Acm)
     symm_eig_solve(Acm, n, w, Vcm, nbw=nbw, nk=nk)
     return w, Vcm.t()
+
+
+def refine(A, n: int, eval, evec, max_iters: int = 2, tol: float = 0.0,
+           stream=None) -> RefineInfo:
+    """Ogita-Aishima refinement in place: ``evec`` (column-major n x n eigenvector columns) is
+    improved against the symmetric ``A`` (column-major, lower triangle read, not modified) and
+    ``eval`` receives the refined eigenvalues.  Returns the step count and measured norms."""
+    _need_f64(A, eval, evec)
+    info = RefineInfo()
+    st = lib().cuev_dsyev_refine(_ptr(A), n, _ptr(eval), _ptr(evec), max_iters, tol,
+                                 _stream(stream), C.byref(info))
+    _check(st, "cuev_dsyev_refine")
+    return info
 
 
 def release_workspace():

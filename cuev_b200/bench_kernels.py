@@ -4,6 +4,7 @@
     python -m cuev_b200.bench_kernels symm M N                   C = A B, A symmetric (lower)
     python -m cuev_b200.bench_kernels syr2k N K                  lower(C) = A B^T + B A^T
     python -m cuev_b200.bench_kernels stages N                   every solver stage on its own
+    python -m cuev_b200.bench_kernels refine N [--iters K]       Ogita-Aishima refinement
 
 `stages` runs the pipeline through the stage entry points (cuev_dbbr_reduce, cuev_bc_chase,
 cuev_tridi_dc, cuev_bc_back, cuev_sbr_back) with an event pair around each, so a profiler can
@@ -127,9 +128,50 @@ def run_stages(a):
         h.close()
 
 
+def run_refine(a):
+    """FP64 solve, eigenvectors rounded to FP32, then K refinement steps against A."""
+    n = a.M
+    A0 = _rand(n, n, 7)
+    A0 = ((A0 + A0.t()) * 0.5).contiguous()
+    A = A0.clone()
+    w = torch.empty(n, dtype=torch.float64, device="cuda")
+    V = torch.empty_like(A0)
+    cv.symm_eig_solve(A, n, w, V)
+    V32 = V.float().double()                       # FP32-accurate start
+    out = {"kernel": "refine", "n": n, "iters": a.iters}
+
+    def metrics(X, lam):
+        Xl = X.t()                                 # column-major storage -> logical matrix
+        R = A0 @ Xl - Xl * lam[None, :]
+        resid = float(torch.linalg.norm(R) / (n * lam.abs().max()))
+        O = Xl.t() @ Xl
+        O.diagonal().sub_(1.0)
+        return resid, float(torch.linalg.norm(O))
+
+    out["start_resid"], out["start_orth"] = metrics(V32, w)
+    times = []
+    for rep in range(a.warmup + a.reps):
+        X = V32.clone()
+        lam = torch.empty_like(w)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        st = torch.cuda.current_stream()
+        e0.record(st)
+        info = cv.refine(A0, n, lam, X, max_iters=a.iters)
+        e1.record(st)
+        torch.cuda.synchronize()
+        if rep >= a.warmup:
+            times.append(e0.elapsed_time(e1))
+    out["ms"] = round(statistics.median(times), 3)
+    out["tflops_7n3_per_step"] = round(7.0 * n ** 3 * a.iters / out["ms"] / 1e9, 3)
+    out["resid"], out["orth"] = metrics(X, lam)
+    out["info"] = {"iterations": info.iterations, "offdiag_fro": info.offdiag_fro,
+                   "orth_fro": info.orth_fro}
+    return out
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
-    ap.add_argument("what", choices=["gemm", "symm", "syr2k", "stages"])
+    ap.add_argument("what", choices=["gemm", "symm", "syr2k", "stages", "refine"])
     ap.add_argument("M", type=int)
     ap.add_argument("N", type=int, nargs="?", default=0)
     ap.add_argument("K", type=int, nargs="?", default=0)
@@ -137,12 +179,14 @@ def main(argv=None):
     ap.add_argument("--tb", type=int, default=0)
     ap.add_argument("--nbw", type=int, default=32)
     ap.add_argument("--nk", type=int, default=0)
+    ap.add_argument("--iters", type=int, default=2)
     ap.add_argument("--reps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=2)
     a = ap.parse_args(argv)
     if a.what == "stages" and a.nk == 0:
         a.nk = 512 if a.M >= 8192 else 256
-    fn = {"gemm": run_gemm, "symm": run_symm, "syr2k": run_syr2k, "stages": run_stages}[a.what]
+    fn = {"gemm": run_gemm, "symm": run_symm, "syr2k": run_syr2k, "stages": run_stages,
+          "refine": run_refine}[a.what]
     print(json.dumps(fn(a)), flush=True)
 
 

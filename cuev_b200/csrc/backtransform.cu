@@ -428,10 +428,15 @@ __global__ void __launch_bounds__(32 * P, 1)
 #pragma unroll
                 for (int i = 0; i < PB; ++i)
                     if (base + i < n) __stcg(Xg + (size_t)(base + i) * 32 + lane, m[i]);
-                __threadfence();
-                __syncwarp();
                 ++oseq;
-                if (lane == 0) sts_release(&S.gprog, oseq);
+                // The first warp of the next round reads these rows almost a whole tile later,
+                // so the device-scope fence (the costliest step of a hop) is paid once per 8 hops
+                // and at the end of the tile.
+                if ((h & 7) == 7 || h == hmax) {
+                    __threadfence();
+                    __syncwarp();
+                    if (lane == 0) sts_release(&S.gprog, oseq);
+                }
             } else {
                 if (!pipe_wait(&S.cons[p], oseq - 1, &S.abort_flag, status, -4)) {
                     ok = false;

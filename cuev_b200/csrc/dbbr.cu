@@ -18,6 +18,7 @@
 #include "solver.cuh"
 
 #include <algorithm>
+#include <cooperative_groups.h>
 
 namespace cuev {
 namespace {
@@ -196,6 +197,173 @@ __global__ void __launch_bounds__(QR_THREADS)
     }
 }
 
+// Cluster variant of the panel QR for panels that fit in the shared memory of one thread-block
+// cluster (up to 16 CTAs of one GPC): the same column loop, but each column's partial dot
+// products are exchanged through distributed shared memory behind one hardware cluster barrier,
+// instead of global partials behind a grid barrier through L2.  Two partial buffers alternate by
+// column parity: a CTA overwrites the buffer of column c-1 only after the cluster barrier of
+// column c, which every CTA reaches after its reads of column c-1.
+template <int BW> size_t panel_qr_cluster_smem(int chunk) {
+    return sizeof(double) * ((size_t)chunk * (BW + 1) + BW * BW + 3 * BW + QR_THREADS + 4 * BW);
+}
+
+template <int BW>
+__global__ void __launch_bounds__(QR_THREADS)
+    panel_qr_cluster_kernel(double *__restrict__ A, long long lda, double *__restrict__ Y,
+                            long long ldy, double *__restrict__ tau, double *__restrict__ T,
+                            double *__restrict__ W, long long ldw, int rows, int b, int chunk,
+                            int *status) {
+    namespace cg = cooperative_groups;
+    constexpr int NRG = QR_THREADS / BW; // row groups
+    constexpr int LD = BW + 1;
+    extern __shared__ __align__(16) double sm[];
+    double *sP = sm;
+    double *sGT = sP + (size_t)chunk * LD;
+    double *sp = sGT + BW * BW;
+    double *srow = sp + BW;
+    double *stau = srow + BW;
+    double *sred = stau + BW;
+    double *spart = sred + QR_THREADS; // [2][BW] this CTA's partial dot products
+    double *sroww = spart + 2 * BW;    // [2][BW] row c of the panel (owner CTA only)
+
+    cg::cluster_group cl = cg::this_cluster();
+    const int tid = threadIdx.x;
+    const int P = (int)cl.num_blocks(), cta = (int)cl.block_rank();
+    const int r0 = cta * chunk;
+    const int cnt = max(0, min(rows, r0 + chunk) - r0);
+    const int j = tid % BW, rg = tid / BW;
+
+    for (int idx = tid; idx < cnt * b; idx += QR_THREADS) {
+        const int r = idx % cnt, c = idx / cnt;
+        sP[r * LD + c] = A[(r0 + r) + (long long)c * lda];
+    }
+    for (int idx = tid; idx < cnt * (BW - b); idx += QR_THREADS) {
+        const int r = idx % cnt, c = b + idx / cnt;
+        sP[r * LD + c] = 0.0;
+    }
+    for (int idx = tid; idx < BW * BW; idx += QR_THREADS) sGT[idx] = 0.0;
+    __syncthreads();
+
+    const int ncols = min(rows, b);
+    for (int c = 0; c < ncols; ++c) {
+        const int buf = c & 1;
+        // (1) partial dots over this CTA's rows strictly below row c
+        double acc = 0.0;
+        const int rstart = max(0, c + 1 - r0);
+        for (int r = rstart + rg; r < cnt; r += NRG) acc += sP[r * LD + c] * sP[r * LD + j];
+        sred[tid] = acc;
+        __syncthreads();
+        if (rg == 0) {
+            double s = 0.0;
+#pragma unroll
+            for (int q = 0; q < NRG; ++q) s += sred[q * BW + j];
+            spart[buf * BW + j] = s;
+            if (c >= r0 && c < r0 + cnt) sroww[buf * BW + j] = sP[(c - r0) * LD + j];
+        }
+        cl.sync();
+
+        // (2) every CTA reduces all partials in the same fixed order (identical results)
+        {
+            double s = 0.0;
+            for (int q = rg; q < P; q += NRG) s += cl.map_shared_rank(spart, q)[buf * BW + j];
+            sred[tid] = s;
+            __syncthreads();
+            if (rg == 0) {
+                double tot = 0.0;
+#pragma unroll
+                for (int q = 0; q < NRG; ++q) tot += sred[q * BW + j];
+                sp[j] = tot;
+                srow[j] = cl.map_shared_rank(sroww, c / chunk)[buf * BW + j];
+            }
+            __syncthreads();
+        }
+
+        // (3) Householder reflector for x = A[c:, c]  (H = I - tau v v^T, v[c] = 1)
+        const double alpha = srow[c];
+        const double s2 = sp[c];
+        double beta = alpha, tauc = 0.0, scal = 0.0;
+        if (s2 > 0.0) {
+            beta = -copysign(hypot(alpha, sqrt(s2)), alpha);
+            tauc = (beta - alpha) / beta;
+            scal = 1.0 / (alpha - beta);
+        }
+        if (!isfinite(s2) || !isfinite(alpha)) {
+            if (tid == 0) dev_fail(status, CUEV_ERR_NONFINITE, c);
+        }
+        // (4) apply H to the trailing columns of own rows (j > c)
+        if (tauc != 0.0) {
+            if (j > c && j < b) {
+                const double wj = srow[j] + scal * sp[j]; // v^T a_j
+                const double f = tauc * wj;
+                for (int r = max(0, c - r0) + rg; r < cnt; r += NRG) {
+                    const int grow = r0 + r;
+                    const double v = (grow == c) ? 1.0 : scal * sP[r * LD + c];
+                    sP[r * LD + j] -= f * v;
+                }
+            }
+        }
+        if (tid < c) sGT[c * BW + tid] = srow[tid] + scal * sp[tid];
+        if (tid == 0) stau[c] = tauc;
+        __syncthreads();
+        // (5) store v_c (scaled) and beta in column c of own rows
+        for (int r = max(0, c - r0) + tid; r < cnt; r += QR_THREADS) {
+            const int grow = r0 + r;
+            if (grow == c)
+                sP[r * LD + c] = beta;
+            else if (grow > c)
+                sP[r * LD + c] *= scal;
+        }
+        __syncthreads();
+    }
+    for (int c = ncols + tid; c < BW; c += QR_THREADS) stau[c] = 0.0;
+    __syncthreads();
+
+    // T: T[c][c] = tau_c,  T[q][c] = -tau_c sum_{p=q}^{c-1} T[q][p] G[p][c]   (q < c)
+    for (int c = 0; c < b; ++c) {
+        if (tid < c) {
+            double s = 0.0;
+            for (int p = tid; p < c; ++p) {
+                const double tqp = (p == tid) ? stau[tid] : sGT[tid * BW + p];
+                s += tqp * sGT[c * BW + p];
+            }
+            sred[tid] = -stau[c] * s;
+        }
+        __syncthreads();
+        if (tid < c) sGT[tid * BW + c] = sred[tid];
+        __syncthreads();
+    }
+
+    for (int idx = tid; idx < cnt * b; idx += QR_THREADS) {
+        const int r = idx % cnt, c = idx / cnt;
+        const int grow = r0 + r;
+        const double a = sP[r * LD + c];
+        A[grow + (long long)c * lda] = a;
+        Y[grow + (long long)c * ldy] = grow > c ? a : (grow == c ? 1.0 : 0.0);
+    }
+    if (W) {
+        for (int idx = tid; idx < cnt * b; idx += QR_THREADS) {
+            const int r = idx % cnt, c = idx / cnt;
+            const int grow = r0 + r;
+            double s = 0.0;
+            const int pmax = min(c, grow);
+            for (int p = 0; p <= pmax; ++p) {
+                const double y = grow > p ? sP[r * LD + p] : 1.0;
+                const double tpc = (p == c) ? stau[c] : sGT[p * BW + c];
+                s += y * tpc;
+            }
+            W[grow + (long long)c * ldw] = s;
+        }
+    }
+    if (cta == 0) {
+        for (int idx = tid; idx < b * b; idx += QR_THREADS) {
+            const int q = idx % b, c = idx / b;
+            T[q + (long long)c * b] = q < c ? sGT[q * BW + c] : (q == c ? stau[c] : 0.0);
+        }
+        for (int c = tid; c < b; c += QR_THREADS) tau[c] = stau[c];
+    }
+    cl.sync(); // no CTA leaves while another may still read its shared memory
+}
+
 // Pack the lower band: B[r + j 2b] = A(j + r, j) for r <= b, 0 for b < r < 2b.
 __global__ void pack_kernel(const double *__restrict__ A, long long lda, double *__restrict__ B,
                             int n, int b) {
@@ -208,6 +376,71 @@ __global__ void pack_kernel(const double *__restrict__ A, long long lda, double 
         const int i = jc + r;
         B[idx] = (r <= b && i < n) ? A[i + (long long)jc * lda] : 0.0;
     }
+}
+
+// Largest cluster the cluster kernel can run with (16 needs the non-portable opt-in; 0 = none),
+// probed once per instantiation with the occupancy API at the full shared-memory size.
+template <int BW> int panel_qr_cluster_max() {
+    static int cached = -1;
+    if (cached >= 0) return cached;
+    cached = 0;
+    auto kern = panel_qr_cluster_kernel<BW>;
+    const size_t smem = max_dynamic_smem((const void *)kern);
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+            cudaSuccess) {
+        cudaGetLastError();
+        return cached;
+    }
+    for (int cl : {16, 8}) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(cl);
+        cfg.blockDim = dim3(QR_THREADS);
+        cfg.dynamicSmemBytes = smem;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = cl, at[0].val.clusterDim.y = 1, at[0].val.clusterDim.z = 1;
+        cfg.attrs = at, cfg.numAttrs = 1;
+        int nclusters = 0;
+        if (cudaOccupancyMaxActiveClusters(&nclusters, (void *)kern, &cfg) == cudaSuccess &&
+            nclusters >= 1) {
+            cached = cl;
+            break;
+        }
+        cudaGetLastError();
+    }
+    return cached;
+}
+
+// Launch the cluster kernel if the panel fits one cluster; returns CUEV_ERR_UNSUPPORTED if not.
+template <int BW> int launch_panel_qr_cluster(Workspace *ws, double *A, long long lda, double *Y,
+                                              long long ldy, double *tau, double *T, double *W,
+                                              long long ldw, int rows, int b) {
+    const int clmax = panel_qr_cluster_max<BW>();
+    if (clmax == 0) return CUEV_ERR_UNSUPPORTED;
+    auto kern = panel_qr_cluster_kernel<BW>;
+    const size_t max_smem = max_dynamic_smem((const void *)kern);
+    int cl = std::max(1, std::min(clmax, div_up(rows, QR_TARGET_ROWS)));
+    int chunk = div_up(rows, cl);
+    while (panel_qr_cluster_smem<BW>(chunk) > max_smem && cl < clmax) {
+        ++cl;
+        chunk = div_up(rows, cl);
+    }
+    if (panel_qr_cluster_smem<BW>(chunk) > max_smem) return CUEV_ERR_UNSUPPORTED;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(cl);
+    cfg.blockDim = dim3(QR_THREADS);
+    cfg.dynamicSmemBytes = panel_qr_cluster_smem<BW>(chunk);
+    cfg.stream = ws->stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = cl, at[0].val.clusterDim.y = 1, at[0].val.clusterDim.z = 1;
+    cfg.attrs = at, cfg.numAttrs = 1;
+    note_launch();
+    CUEV_TRY(cudaLaunchKernelEx(&cfg, kern, A, lda, Y, ldy, tau, T, W, ldw, rows, b, chunk,
+                                ws->status));
+    return CUEV_OK;
 }
 
 template <int BW> int launch_panel_qr(Workspace *ws, double *A, long long lda, double *Y,
@@ -253,8 +486,16 @@ template <int BW> int launch_panel_qr(Workspace *ws, double *A, long long lda, d
 int panel_qr(Workspace *ws, double *A, long long lda, double *Y, long long ldy, double *tau,
              double *T, double *W, long long ldw, int rows, int b) {
     if (rows <= 0 || b <= 0) return CUEV_OK;
-    if (b <= 32) return launch_panel_qr<32>(ws, A, lda, Y, ldy, tau, T, W, ldw, rows, b);
-    if (b <= 64) return launch_panel_qr<64>(ws, A, lda, Y, ldy, tau, T, W, ldw, rows, b);
+    if (b <= 32) {
+        const int st = launch_panel_qr_cluster<32>(ws, A, lda, Y, ldy, tau, T, W, ldw, rows, b);
+        if (st != CUEV_ERR_UNSUPPORTED) return st;
+        return launch_panel_qr<32>(ws, A, lda, Y, ldy, tau, T, W, ldw, rows, b);
+    }
+    if (b <= 64) {
+        const int st = launch_panel_qr_cluster<64>(ws, A, lda, Y, ldy, tau, T, W, ldw, rows, b);
+        if (st != CUEV_ERR_UNSUPPORTED) return st;
+        return launch_panel_qr<64>(ws, A, lda, Y, ldy, tau, T, W, ldw, rows, b);
+    }
     set_last_message("panel QR supports b <= 64");
     return CUEV_ERR_INVALID;
 }

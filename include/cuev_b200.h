@@ -85,6 +85,21 @@ int cuev_dsyev_adjoint(const double *V, const double *lam, const double *Vbar,
 int cuev_ssyev_adjoint(const float *V, const float *lam, const float *Vbar, const float *lambar,
                        int n, float gap_tol, float *Abar, void *stream);
 
+/* Precision form, refinement half (no reference counterpart): Ogita-Aishima iterative
+ * refinement of an approximate eigendecomposition of the symmetric A (n x n, lower triangle
+ * read, not modified).  evec (n x n, columns) is improved in place and eval receives the refined
+ * eigenvalues.  Each step costs 7 n^3 FP64 flop; the step measures ||I - X^T X||_F and
+ * ||X^T A X - diag(lam)||_F first and stops early once both are <= tol (relative to max|lam| for
+ * the second; tol <= 0 runs all max_iters steps).  info may be NULL.  Blocks until done. */
+typedef struct cuev_refine_info {
+    int iterations;     /* refinement steps applied */
+    double offdiag_fro; /* ||X^T A X - diag(lam)||_F of the last X measured */
+    double orth_fro;    /* ||I - X^T X||_F of the last X measured */
+    double anorm;       /* max |lam_i|, the ||A||_2 estimate */
+} cuev_refine_info;
+int cuev_dsyev_refine(const double *A, int n, double *eval, double *evec, int max_iters,
+                      double tol, void *stream, cuev_refine_info *info);
+
 /* Release the cached device workspace (the solves keep one pool per (n, b, k) between calls). */
 int cuev_release_workspace(void);
 

@@ -493,6 +493,32 @@ def symm_eig_solve(A0: np.ndarray, b: int = 32, k: int = 512, timings: dict | No
 
 
 # ------------------------------------------------------------------------------------------
+# Precision form: Ogita-Aishima refinement (no reference counterpart; restates Algorithm 1 of
+# T. Ogita, K. Aishima, Japan J. Indust. Appl. Math. 35 (2018) with the same Frobenius-norm
+# threshold as cuev_b200/csrc/refine.cu)
+# ------------------------------------------------------------------------------------------
+def refine_ogita_aishima(A: np.ndarray, X: np.ndarray, steps: int):
+    """Returns (lam, X) after `steps` refinement steps of the symmetric A (full matrix)."""
+    X = np.array(X, dtype=np.float64, copy=True)
+    lam = None
+    for _ in range(steps):
+        G = X.T @ X
+        S = X.T @ (A @ X)
+        S = 0.5 * (S + S.T)                            # symmetric part, as the GPU step
+        lam = np.diag(S) / np.diag(G)
+        R = np.eye(X.shape[0]) - G
+        off = S - np.diag(lam)
+        delta = 2.0 * (np.linalg.norm(off) + np.abs(lam).max() * np.linalg.norm(R))
+        gap = lam[None, :] - lam[:, None]              # gap[i, j] = lam_j - lam_i
+        far = np.abs(gap) > delta
+        with np.errstate(divide="ignore", invalid="ignore"):
+            E = np.where(far, (S + lam[None, :] * R) / np.where(far, gap, 1.0), 0.5 * R)
+        np.fill_diagonal(E, 0.5 * np.diag(R))
+        X = X + X @ E
+    return lam, X
+
+
+# ------------------------------------------------------------------------------------------
 # Metrics (both normalisations used by the reference and the build)
 # ------------------------------------------------------------------------------------------
 def metrics(A: np.ndarray, w: np.ndarray, V: np.ndarray, w_ref: np.ndarray | None = None):
