@@ -25,6 +25,7 @@ namespace {
 
 constexpr int QR_THREADS = 256;
 constexpr int QR_TARGET_ROWS = 128; // rows per CTA the launcher aims for
+constexpr int QRC_THREADS = 512;    // cluster variant: up to ~800 rows per CTA
 
 // Shared-memory layout of panel_qr_kernel<BW>:
 //   sP  [chunk][BW + 1]  this CTA's rows of the panel
@@ -204,17 +205,17 @@ __global__ void __launch_bounds__(QR_THREADS)
 // column parity: a CTA overwrites the buffer of column c-1 only after the cluster barrier of
 // column c, which every CTA reaches after its reads of column c-1.
 template <int BW> size_t panel_qr_cluster_smem(int chunk) {
-    return sizeof(double) * ((size_t)chunk * (BW + 1) + BW * BW + 3 * BW + QR_THREADS + 4 * BW);
+    return sizeof(double) * ((size_t)chunk * (BW + 1) + BW * BW + 3 * BW + QRC_THREADS + 4 * BW);
 }
 
 template <int BW>
-__global__ void __launch_bounds__(QR_THREADS)
+__global__ void __launch_bounds__(QRC_THREADS)
     panel_qr_cluster_kernel(double *__restrict__ A, long long lda, double *__restrict__ Y,
                             long long ldy, double *__restrict__ tau, double *__restrict__ T,
                             double *__restrict__ W, long long ldw, int rows, int b, int chunk,
                             int *status) {
     namespace cg = cooperative_groups;
-    constexpr int NRG = QR_THREADS / BW; // row groups
+    constexpr int NRG = QRC_THREADS / BW; // row groups
     constexpr int LD = BW + 1;
     extern __shared__ __align__(16) double sm[];
     double *sP = sm;
@@ -223,7 +224,7 @@ __global__ void __launch_bounds__(QR_THREADS)
     double *srow = sp + BW;
     double *stau = srow + BW;
     double *sred = stau + BW;
-    double *spart = sred + QR_THREADS; // [2][BW] this CTA's partial dot products
+    double *spart = sred + QRC_THREADS; // [2][BW] this CTA's partial dot products
     double *sroww = spart + 2 * BW;    // [2][BW] row c of the panel (owner CTA only)
 
     cg::cluster_group cl = cg::this_cluster();
@@ -233,25 +234,32 @@ __global__ void __launch_bounds__(QR_THREADS)
     const int cnt = max(0, min(rows, r0 + chunk) - r0);
     const int j = tid % BW, rg = tid / BW;
 
-    for (int idx = tid; idx < cnt * b; idx += QR_THREADS) {
+    for (int idx = tid; idx < cnt * b; idx += QRC_THREADS) {
         const int r = idx % cnt, c = idx / cnt;
         sP[r * LD + c] = A[(r0 + r) + (long long)c * lda];
     }
-    for (int idx = tid; idx < cnt * (BW - b); idx += QR_THREADS) {
+    for (int idx = tid; idx < cnt * (BW - b); idx += QRC_THREADS) {
         const int r = idx % cnt, c = b + idx / cnt;
         sP[r * LD + c] = 0.0;
     }
-    for (int idx = tid; idx < BW * BW; idx += QR_THREADS) sGT[idx] = 0.0;
+    for (int idx = tid; idx < BW * BW; idx += QRC_THREADS) sGT[idx] = 0.0;
     __syncthreads();
 
     const int ncols = min(rows, b);
     for (int c = 0; c < ncols; ++c) {
         const int buf = c & 1;
         // (1) partial dots over this CTA's rows strictly below row c
-        double acc = 0.0;
-        const int rstart = max(0, c + 1 - r0);
-        for (int r = rstart + rg; r < cnt; r += NRG) acc += sP[r * LD + c] * sP[r * LD + j];
-        sred[tid] = acc;
+        // four independent chains: a CTA holds up to ~800 rows, 50 per thread and column
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+        int r = max(0, c + 1 - r0) + rg;
+        for (; r + 3 * NRG < cnt; r += 4 * NRG) {
+            a0 = fma(sP[r * LD + c], sP[r * LD + j], a0);
+            a1 = fma(sP[(r + NRG) * LD + c], sP[(r + NRG) * LD + j], a1);
+            a2 = fma(sP[(r + 2 * NRG) * LD + c], sP[(r + 2 * NRG) * LD + j], a2);
+            a3 = fma(sP[(r + 3 * NRG) * LD + c], sP[(r + 3 * NRG) * LD + j], a3);
+        }
+        for (; r < cnt; r += NRG) a0 = fma(sP[r * LD + c], sP[r * LD + j], a0);
+        sred[tid] = (a0 + a1) + (a2 + a3);
         __syncthreads();
         if (rg == 0) {
             double s = 0.0;
@@ -295,6 +303,7 @@ __global__ void __launch_bounds__(QR_THREADS)
             if (j > c && j < b) {
                 const double wj = srow[j] + scal * sp[j]; // v^T a_j
                 const double f = tauc * wj;
+#pragma unroll 4
                 for (int r = max(0, c - r0) + rg; r < cnt; r += NRG) {
                     const int grow = r0 + r;
                     const double v = (grow == c) ? 1.0 : scal * sP[r * LD + c];
@@ -306,7 +315,7 @@ __global__ void __launch_bounds__(QR_THREADS)
         if (tid == 0) stau[c] = tauc;
         __syncthreads();
         // (5) store v_c (scaled) and beta in column c of own rows
-        for (int r = max(0, c - r0) + tid; r < cnt; r += QR_THREADS) {
+        for (int r = max(0, c - r0) + tid; r < cnt; r += QRC_THREADS) {
             const int grow = r0 + r;
             if (grow == c)
                 sP[r * LD + c] = beta;
@@ -315,7 +324,7 @@ __global__ void __launch_bounds__(QR_THREADS)
         }
         __syncthreads();
     }
-    for (int c = ncols + tid; c < BW; c += QR_THREADS) stau[c] = 0.0;
+    for (int c = ncols + tid; c < BW; c += QRC_THREADS) stau[c] = 0.0;
     __syncthreads();
 
     // T: T[c][c] = tau_c,  T[q][c] = -tau_c sum_{p=q}^{c-1} T[q][p] G[p][c]   (q < c)
@@ -333,7 +342,7 @@ __global__ void __launch_bounds__(QR_THREADS)
         __syncthreads();
     }
 
-    for (int idx = tid; idx < cnt * b; idx += QR_THREADS) {
+    for (int idx = tid; idx < cnt * b; idx += QRC_THREADS) {
         const int r = idx % cnt, c = idx / cnt;
         const int grow = r0 + r;
         const double a = sP[r * LD + c];
@@ -341,7 +350,7 @@ __global__ void __launch_bounds__(QR_THREADS)
         Y[grow + (long long)c * ldy] = grow > c ? a : (grow == c ? 1.0 : 0.0);
     }
     if (W) {
-        for (int idx = tid; idx < cnt * b; idx += QR_THREADS) {
+        for (int idx = tid; idx < cnt * b; idx += QRC_THREADS) {
             const int r = idx % cnt, c = idx / cnt;
             const int grow = r0 + r;
             double s = 0.0;
@@ -355,11 +364,11 @@ __global__ void __launch_bounds__(QR_THREADS)
         }
     }
     if (cta == 0) {
-        for (int idx = tid; idx < b * b; idx += QR_THREADS) {
+        for (int idx = tid; idx < b * b; idx += QRC_THREADS) {
             const int q = idx % b, c = idx / b;
             T[q + (long long)c * b] = q < c ? sGT[q * BW + c] : (q == c ? stau[c] : 0.0);
         }
-        for (int c = tid; c < b; c += QR_THREADS) tau[c] = stau[c];
+        for (int c = tid; c < b; c += QRC_THREADS) tau[c] = stau[c];
     }
     cl.sync(); // no CTA leaves while another may still read its shared memory
 }
@@ -396,7 +405,7 @@ template <int BW> int panel_qr_cluster_max() {
     for (int cl : {16, 8}) {
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(cl);
-        cfg.blockDim = dim3(QR_THREADS);
+        cfg.blockDim = dim3(QRC_THREADS);
         cfg.dynamicSmemBytes = smem;
         cudaLaunchAttribute at[1];
         at[0].id = cudaLaunchAttributeClusterDimension;
@@ -430,7 +439,7 @@ template <int BW> int launch_panel_qr_cluster(Workspace *ws, double *A, long lon
     if (panel_qr_cluster_smem<BW>(chunk) > max_smem) return CUEV_ERR_UNSUPPORTED;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(cl);
-    cfg.blockDim = dim3(QR_THREADS);
+    cfg.blockDim = dim3(QRC_THREADS);
     cfg.dynamicSmemBytes = panel_qr_cluster_smem<BW>(chunk);
     cfg.stream = ws->stream;
     cudaLaunchAttribute at[1];

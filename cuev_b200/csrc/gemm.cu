@@ -7,24 +7,29 @@
 namespace cuev {
 namespace {
 
-constexpr int BK = 16; // k-depth of one shared-memory stage (4 DMMA k-steps)
 constexpr int PAD = 4; // row padding (doubles): keeps fragment reads bank-conflict free
 
 // KS_: k-depth of one DMMA (8 or 16); the k16 shape needs twice the fragment registers.
-template <int BM_, int BN_, int WARPS_M_, int WARPS_N_, int STAGES_, int KS_ = 16> struct TileCfg {
+// BK_: k-depth of one shared-memory stage (a multiple of KS_).
+template <int BM_, int BN_, int WARPS_M_, int WARPS_N_, int STAGES_, int KS_ = 16, int BK_ = 16>
+struct TileCfg {
     static constexpr int BM = BM_, BN = BN_, WARPS_M = WARPS_M_, WARPS_N = WARPS_N_;
-    static constexpr int STAGES = STAGES_, KS = KS_;
+    static constexpr int STAGES = STAGES_, KS = KS_, BK = BK_;
+    static_assert(BK % KS == 0 && BK % 16 == 0, "stage depth");
     static_assert(KS == 8 || KS == 16, "DMMA k-depth");
     static constexpr int NT = 32 * WARPS_M * WARPS_N;
     static constexpr int WM = BM / WARPS_M, WN = BN / WARPS_N;
     static constexpr int MT = WM / 16, NTL = WN / 8;
     static_assert(WM % 16 == 0 && WN % 8 == 0, "warp tile must be a multiple of the DMMA shape");
+    // every thread copies a whole number (>= 1) of 16-byte pairs of each operand tile per stage
+    static_assert((BM / 2) * BK % NT == 0 && (BM / 2) * BK / NT >= 1, "A tile / threads");
+    static_assert((BN / 2) * BK % NT == 0 && (BN / 2) * BK / NT >= 1, "B tile / threads");
 };
 
 using CfgBig = TileCfg<128, 128, 4, 4, 4, 8>; // 16 warps: two per SMSP left the DMMA pipe idle
 using CfgSkinny = TileCfg<128, 64, 4, 2, 4>;
 using CfgSmall = TileCfg<64, 64, 2, 2, 4>;
-using CfgN32 = TileCfg<256, 32, 8, 1, 4>; // N <= 32 (band width 32 panels)
+using CfgN32 = TileCfg<128, 32, 8, 1, 4>; // N <= 32 (band width 32 panels): 16 x 32 warp tiles
 
 __device__ __forceinline__ void cp_async8(double *smem, const double *gmem, bool pred) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -66,6 +71,7 @@ __device__ __forceinline__ void dmma16x8x16(double (&d)[4], const double (&a)[8]
 }
 
 template <class C, bool TA, bool TB, bool SYMM> struct SmemLayout {
+    static constexpr int BK = C::BK;
     // "outer-contiguous" tiles are stored [k][outer] (the global matrix is contiguous along the
     // outer index), the others [outer][k].
     static constexpr bool A_OUTER = SYMM || !TA;
@@ -86,6 +92,7 @@ template <class C, bool TA, bool TB, bool SYMM, bool BATCHED, int VEC>
 __global__ void __launch_bounds__(C::NT)
     dgemm_kernel(const GemmArgs args_val, const GemmArgs *__restrict__ args_arr) {
     using L = SmemLayout<C, TA, TB, SYMM>;
+    constexpr int BK = C::BK;
     extern __shared__ __align__(16) double smem[];
 
     const GemmArgs a = BATCHED ? args_arr[blockIdx.z] : args_val;
