@@ -76,6 +76,7 @@ _SIGS = {
     "cuev_dbbr_pack": [_VP, _DP, _DP],
     "cuev_bc_chase": [_VP, _DP, _DP, _DP],
     "cuev_tridi_dc": [_VP, _DP, _DP, _DP, _DP],
+    "cuev_tridi_eigvals": [_VP, _DP, _DP, _DP],
     "cuev_bc_back": [_VP, _DP, _I],
     "cuev_sbr_back": [_VP, _DP, _I],
     "cuev_back_transform": [_VP, _DP, C.POINTER(Timer)],
@@ -196,6 +197,17 @@ def refine(A, n: int, eval, evec, max_iters: int = 2, tol: float = 0.0,
     return info
 
 
+def eigvalsh(A_rowmajor_sym, nbw: int = 0, nk: int = 0):
+    """Eigenvalues only (ascending) of a symmetric torch matrix: band reduction, bulge chase and
+    bisection, no eigenvectors.  Uses the lower triangle."""
+    import torch
+    n = A_rowmajor_sym.shape[0]
+    Acm = A_rowmajor_sym.t().contiguous().clone()
+    w = torch.empty(n, dtype=Acm.dtype, device=Acm.device)
+    symm_eig_solve(Acm, n, w, None, nbw=nbw, nk=nk)
+    return w
+
+
 def release_workspace():
     _check(lib().cuev_release_workspace(), "cuev_release_workspace")
 
@@ -258,6 +270,9 @@ class SolverHandle:
     def tridi_dc(self, d, e, eval, evec):
         _check(lib().cuev_tridi_dc(self.h, _ptr(d), _ptr(e), _ptr(eval), _ptr(evec)),
                "tridi_dc")
+
+    def tridi_eigvals(self, d, e, eval):
+        _check(lib().cuev_tridi_eigvals(self.h, _ptr(d), _ptr(e), _ptr(eval)), "tridi_eigvals")
 
     def bc_back(self, M, ldm):
         _check(lib().cuev_bc_back(self.h, _ptr(M), ldm), "bc_back")

@@ -5,6 +5,8 @@
     python -m cuev_b200.bench_kernels syr2k N K                  lower(C) = A B^T + B A^T
     python -m cuev_b200.bench_kernels stages N                   every solver stage on its own
     python -m cuev_b200.bench_kernels refine N [--iters K]       Ogita-Aishima refinement
+    python -m cuev_b200.bench_kernels eigvals N                  eigenvalues-only solve
+    python -m cuev_b200.bench_kernels adjoint N                  eigh forward + adjoint
 
 `stages` runs the pipeline through the stage entry points (cuev_dbbr_reduce, cuev_bc_chase,
 cuev_tridi_dc, cuev_bc_back, cuev_sbr_back) with an event pair around each, so a profiler can
@@ -169,9 +171,73 @@ def run_refine(a):
     return out
 
 
+def run_eigvals(a):
+    """Eigenvalues-only solve (evec = NULL) through the C ABI, with the per-stage timer."""
+    n = a.M
+    A0 = _rand(n, n, 7)
+    A0 = ((A0 + A0.t()) * 0.5).contiguous()
+    A = torch.empty_like(A0)
+    w = torch.empty(n, dtype=torch.float64, device="cuda")
+    t = cv.Timer()
+    times, stages = [], []
+    for rep in range(a.warmup + a.reps):
+        A.copy_(A0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        st = torch.cuda.current_stream()
+        e0.record(st)
+        cv.symm_eig_solve(A, n, w, None, timer=t, nbw=a.nbw, nk=a.nk)
+        e1.record(st)
+        torch.cuda.synchronize()
+        if rep >= a.warmup:
+            times.append(e0.elapsed_time(e1))
+            stages.append(t.as_dict())
+    med = statistics.median(times)
+    last = stages[-1]
+    return {"kernel": "eigvals_only_solve", "n": n, "nbw": a.nbw, "nk": a.nk,
+            "ms": round(med, 3), "dbbr_ms": round(last["dbbr_ms"], 3),
+            "bc_ms": round(last["bc_ms"], 3), "bisection_ms": round(last["dc_ms"], 3)}
+
+
+def run_adjoint(a):
+    """Forward solve plus the adjoint (cuev_dsyev_adjoint) for seeded cotangents: the
+    differentiation form's forward + backward time."""
+    import ctypes as C
+    n = a.M
+    A0 = _rand(n, n, 7)
+    A0 = ((A0 + A0.t()) * 0.5).contiguous()
+    A = torch.empty_like(A0)
+    w = torch.empty(n, dtype=torch.float64, device="cuda")
+    V = torch.empty_like(A0)
+    gw = _rand(1, n, 8).reshape(n)
+    gV = _rand(n, n, 9)
+    Abar = torch.empty_like(A0)
+    L = cv.lib()
+    st = torch.cuda.current_stream()
+    fwd, bwd = [], []
+    for rep in range(a.warmup + a.reps):
+        A.copy_(A0)
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        e[0].record(st)
+        cv.symm_eig_solve(A, n, w, V, nbw=a.nbw, nk=a.nk)
+        e[1].record(st)
+        r = L.cuev_dsyev_adjoint(V.data_ptr(), w.data_ptr(), gV.data_ptr(), gw.data_ptr(), n,
+                                 C.c_double(1e-12), Abar.data_ptr(), st.cuda_stream)
+        cv._check(r, "cuev_dsyev_adjoint")
+        e[2].record(st)
+        torch.cuda.synchronize()
+        if rep >= a.warmup:
+            fwd.append(e[0].elapsed_time(e[1]))
+            bwd.append(e[1].elapsed_time(e[2]))
+    f, b = statistics.median(fwd), statistics.median(bwd)
+    return {"kernel": "eigh_fwd_bwd", "n": n, "fwd_ms": round(f, 3), "bwd_ms": round(b, 3),
+            "fwd_bwd_ms": round(f + b, 3),
+            "bwd_tflops_6n3": round(6.0 * n ** 3 / b / 1e9, 3)}
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
-    ap.add_argument("what", choices=["gemm", "symm", "syr2k", "stages", "refine"])
+    ap.add_argument("what", choices=["gemm", "symm", "syr2k", "stages", "refine", "eigvals",
+                                     "adjoint"])
     ap.add_argument("M", type=int)
     ap.add_argument("N", type=int, nargs="?", default=0)
     ap.add_argument("K", type=int, nargs="?", default=0)
@@ -183,10 +249,10 @@ def main(argv=None):
     ap.add_argument("--reps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=2)
     a = ap.parse_args(argv)
-    if a.what == "stages" and a.nk == 0:
+    if a.what in ("stages", "eigvals", "adjoint") and a.nk == 0:
         a.nk = 512 if a.M >= 8192 else 256
     fn = {"gemm": run_gemm, "symm": run_symm, "syr2k": run_syr2k, "stages": run_stages,
-          "refine": run_refine}[a.what]
+          "refine": run_refine, "eigvals": run_eigvals, "adjoint": run_adjoint}[a.what]
     print(json.dumps(fn(a)), flush=True)
 
 

@@ -84,7 +84,7 @@ __global__ void nonfinite_scan_kernel(const double *__restrict__ A, int n, long 
 
 __global__ void small_solve_kernel(const double *A, double *eval, double *evec) {
     eval[0] = A[0];
-    evec[0] = 1.0;
+    if (evec) evec[0] = 1.0;
 }
 
 struct EventSet {
@@ -105,7 +105,7 @@ int solve_d(double *A, int n, double *eval, double *evec, cudaStream_t stream, c
             const cuev_config *cfg) {
     if (n < 0) return CUEV_ERR_INVALID;
     if (n == 0) return CUEV_OK;
-    if (!A || !eval || !evec) return CUEV_ERR_INVALID;
+    if (!A || !eval) return CUEV_ERR_INVALID; // evec == NULL: eigenvalues only
     auto wall0 = std::chrono::high_resolution_clock::now();
     if (n == 1) {
         small_solve_kernel<<<1, 1, 0, stream>>>(A, eval, evec); note_launch();
@@ -140,11 +140,17 @@ int solve_d(double *A, int n, double *eval, double *evec, cudaStream_t stream, c
     CUEV_CHECK_STATUS(rec(1));
     CUEV_CHECK_STATUS(bc_chase(ws, ws->B, ws->d, ws->e));
     CUEV_CHECK_STATUS(rec(2));
-    CUEV_CHECK_STATUS(tridi_dc(ws, ws->d, ws->e, eval, evec));
-    CUEV_CHECK_STATUS(rec(3));
-    CUEV_CHECK_STATUS(bc_back(ws, evec, n));
-    CUEV_CHECK_STATUS(rec(4));
-    CUEV_CHECK_STATUS(sbr_back(ws, evec, n));
+    if (evec) {
+        CUEV_CHECK_STATUS(tridi_dc(ws, ws->d, ws->e, eval, evec));
+        CUEV_CHECK_STATUS(rec(3));
+        CUEV_CHECK_STATUS(bc_back(ws, evec, n));
+        CUEV_CHECK_STATUS(rec(4));
+        CUEV_CHECK_STATUS(sbr_back(ws, evec, n));
+    } else { // eigenvalues only: bisection replaces D&C, no back-transform
+        CUEV_CHECK_STATUS(tridi_eigvals(ws, ws->d, ws->e, eval));
+        CUEV_CHECK_STATUS(rec(3));
+        CUEV_CHECK_STATUS(rec(4));
+    }
     CUEV_CHECK_STATUS(rec(5));
     CUEV_CHECK_STATUS(workspace_check_status(ws, "solve"));
     auto wall1 = std::chrono::high_resolution_clock::now();
@@ -158,6 +164,7 @@ int solve_d(double *A, int n, double *eval, double *evec, cudaStream_t stream, c
         timer->bt_qb_ms = t[3];
         timer->bt_qs_ms = t[4];
         timer->bt_ms = t[3] + t[4];
+        if (!evec) timer->bt_qb_ms = timer->bt_qs_ms = timer->bt_ms = 0.0f; // not run
         timer->total_ms = std::chrono::duration<float, std::milli>(wall1 - wall0).count();
     }
     return CUEV_OK;
@@ -193,7 +200,7 @@ extern "C" int cuev_ssyevd(float *A, int n, float *eval, float *evec, void *stre
                            cuev_timer *timer) {
     if (n < 0) return CUEV_ERR_INVALID;
     if (n == 0) return CUEV_OK;
-    if (!A || !eval || !evec) return CUEV_ERR_INVALID;
+    if (!A || !eval) return CUEV_ERR_INVALID; // evec == NULL: eigenvalues only
     cudaStream_t st = (cudaStream_t)stream;
     const long long nn = (long long)n * n;
     double *buf = nullptr;
@@ -205,9 +212,9 @@ extern "C" int cuev_ssyevd(float *A, int n, float *eval, float *evec, void *stre
     double *A64 = buf, *V64 = buf + nn, *w64 = buf + 2 * nn;
     const int blocks = 4 * num_sms();
     widen_kernel<<<blocks, 256, 0, st>>>(A, A64, nn); note_launch();
-    int s = solve_d(A64, n, w64, V64, st, timer, nullptr);
+    int s = solve_d(A64, n, w64, evec ? V64 : nullptr, st, timer, nullptr);
     if (s == CUEV_OK) {
-        narrow_kernel<<<blocks, 256, 0, st>>>(V64, evec, nn); note_launch();
+        if (evec) { narrow_kernel<<<blocks, 256, 0, st>>>(V64, evec, nn); note_launch(); }
         narrow_kernel<<<1, 256, 0, st>>>(w64, eval, n); note_launch();
         narrow_kernel<<<blocks, 256, 0, st>>>(A64, A, nn); note_launch(); // A is clobbered like the reference's
     }
@@ -305,6 +312,13 @@ extern "C" int cuev_tridi_dc(cuev_handle h, const double *d, const double *e, do
     if (!d || !e || !eval || !evec) return CUEV_ERR_INVALID;
     CUEV_CHECK_STATUS(tridi_dc(h->ws, d, e, eval, evec));
     return workspace_check_status(h->ws, "tridi_dc");
+}
+
+extern "C" int cuev_tridi_eigvals(cuev_handle h, const double *d, const double *e, double *eval) {
+    HCHECK(h);
+    if (!d || !e || !eval) return CUEV_ERR_INVALID;
+    CUEV_CHECK_STATUS(tridi_eigvals(h->ws, d, e, eval));
+    return workspace_check_status(h->ws, "tridi_eigvals");
 }
 
 extern "C" int cuev_bc_back(cuev_handle h, double *M, int ldm) {

@@ -26,7 +26,9 @@ struct TileCfg {
     static_assert((BN / 2) * BK % NT == 0 && (BN / 2) * BK / NT >= 1, "B tile / threads");
 };
 
-using CfgBig = TileCfg<128, 128, 4, 4, 4, 8>; // 16 warps: two per SMSP left the DMMA pipe idle
+using CfgBig = TileCfg<128, 128, 4, 4, 3, 8, 32>; // 16 warps (two per SMSP left the DMMA pipe idle), BK 32
+// batched (D&C merge) problems read with 8-byte copies, where 32-deep stages are slower
+using CfgBigBatched = TileCfg<128, 128, 4, 4, 4, 8>;
 using CfgSkinny = TileCfg<128, 64, 4, 2, 4>;
 using CfgSmall = TileCfg<64, 64, 2, 2, 4>;
 using CfgN32 = TileCfg<128, 32, 8, 1, 4>; // N <= 32 (band width 32 panels): 16 x 32 warp tiles
@@ -554,7 +556,7 @@ int gemm_batched_launch(const GemmArgs *dev_args, int count, int max_m, int max_
         int st;
         switch (tl) {
         case Tile::Big:
-            st = dispatch_t<CfgBig, false, true>(dummy, dev_args + z0, ta, tb, grid, stream);
+            st = dispatch_t<CfgBigBatched, false, true>(dummy, dev_args + z0, ta, tb, grid, stream);
             break;
         case Tile::Skinny:
             st = dispatch_t<CfgSkinny, false, true>(dummy, dev_args + z0, ta, tb, grid, stream);

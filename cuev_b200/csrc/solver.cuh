@@ -75,6 +75,8 @@ int bc_chase(Workspace *ws, double *B, double *d, double *e);
 
 // Stage 3: tridiagonal divide and conquer (tridi.cu)
 int tridi_dc(Workspace *ws, const double *d, const double *e, double *eval, double *evec);
+// Eigenvalues only of the tridiagonal (bisection; tridi_eigvals.cu).
+int tridi_eigvals(Workspace *ws, const double *d, const double *e, double *eval);
 
 // Stage 4: back-transform (backtransform.cu)
 int bc_back(Workspace *ws, double *M, long long ldm);

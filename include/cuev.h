@@ -37,7 +37,8 @@ struct SolveTimer {
  * @param[in,out] A      n x n symmetric matrix (column-major, lower triangle read), overwritten
  * @param[in]     n      matrix dimension
  * @param[out]    eval   eigenvalues in ascending order, length n
- * @param[out]    evec   eigenvectors as columns, n x n (column-major)
+ * @param[out]    evec   eigenvectors as columns, n x n (column-major); may be nullptr here
+ *                       (eigenvalues only, an extension over the reference)
  * @param[in]     stream CUDA stream
  * @param[out]    timer  optional per-stage timing breakdown
  */

@@ -61,7 +61,9 @@ typedef struct cuev_config {
  * ------------------------------------------------------------------------------------------ */
 
 /* Plain FP64 solve.  Replaces cuev::symm_eig_solve<double> (reference src/cuda/solver.cu:25-73,
- * instantiated at :79).  timer may be NULL. */
+ * instantiated at :79).  timer may be NULL.  evec may be NULL (no reference counterpart: the
+ * reference always forms eigenvectors): then only the eigenvalues are computed, by bisection on
+ * the tridiagonal after the band reduction and bulge chase, with no D&C and no back-transform. */
 int cuev_dsyevd(double *A, int n, double *eval, double *evec, void *stream, cuev_timer *timer);
 
 /* Same with explicit blocking (reference: handle_alloc(n, nbw, nk, stream),
@@ -156,6 +158,11 @@ int cuev_bc_chase(cuev_handle h, double *B, double *d, double *e);
  * tridiagonal (n x n, ld n).  d and e are not modified.  Replaces kernels::tridi_dc (reference
  * src/cuda/tridi.cu:425-452, a host LAPACK D&C). */
 int cuev_tridi_dc(cuev_handle h, const double *d, const double *e, double *eval, double *evec);
+
+/* Eigenvalues only of the tridiagonal (d, e), ascending, by bisection on Sturm counts (one thread
+ * per eigenvalue).  No reference counterpart: the stage the eigenvalues-only solve (evec == NULL)
+ * runs in place of cuev_tridi_dc. */
+int cuev_tridi_eigvals(cuev_handle h, const double *d, const double *e, double *eval);
 
 /* M <- Q_b M (n x n, ld ldm).  Replaces kernels::bc_back (reference src/cuda/backtransform.cu:183-207). */
 int cuev_bc_back(cuev_handle h, double *M, int ldm);

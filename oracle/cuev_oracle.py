@@ -493,6 +493,17 @@ def symm_eig_solve(A0: np.ndarray, b: int = 32, k: int = 512, timings: dict | No
 
 
 # ------------------------------------------------------------------------------------------
+# Eigenvalues only of a tridiagonal (no reference counterpart: the reference always forms
+# eigenvectors).  LAPACK's tridiagonal eigenvalue driver through scipy.
+# ------------------------------------------------------------------------------------------
+def tridi_eigvals(d: np.ndarray, e: np.ndarray) -> np.ndarray:
+    import scipy.linalg as sla
+    if d.size == 0:
+        return np.zeros(0)
+    return sla.eigvalsh_tridiagonal(np.asarray(d, float), np.asarray(e, float))
+
+
+# ------------------------------------------------------------------------------------------
 # Precision form: Ogita-Aishima refinement (no reference counterpart; restates Algorithm 1 of
 # T. Ogita, K. Aishima, Japan J. Indust. Appl. Math. 35 (2018) with the same Frobenius-norm
 # threshold as cuev_b200/csrc/refine.cu)

@@ -77,6 +77,44 @@ def test_clustered_spectrum(cuda):
     assert m["orth_fro"] / np.sqrt(n) < 1e-13, m
 
 
+@pytest.mark.parametrize("nbw", [64, 32])
+def test_config2_full_size(cuda, nbw):
+    """Config C2 at full size: n = 8192, A = Q diag(lam) Q^T with Q from the QR of a seeded
+    Gaussian, half of lam in 64 clusters of 64 (members centre * (1 + 1e-10 U(-1, 1)), centres
+    log-uniform on [1e-6, 1]) and half log-uniform on [1e-6, 1]; k = 512.  The exact spectrum is
+    known, so the eigenvalues are checked against it (the matrix is formed on the GPU in FP64)."""
+    import torch
+    import cuev_b200 as cv
+    n = 8192
+    rng = np.random.default_rng(8192)
+    centres = 10.0 ** rng.uniform(-6, 0, 64)
+    cl = np.concatenate([c * (1 + 1e-10 * rng.uniform(-1, 1, 64)) for c in centres])
+    rest = 10.0 ** rng.uniform(-6, 0, n - cl.size)
+    lam = rng.permutation(np.concatenate([cl, rest]))
+    G = torch.from_numpy(rng.standard_normal((n, n))).to(cuda)
+    Q, _ = torch.linalg.qr(G)
+    del G
+    lt = torch.from_numpy(lam).to(cuda)
+    A = (Q * lt[None, :]) @ Q.t()
+    A = (A + A.t()) * 0.5                        # symmetric: row- and column-major storage agree
+    del Q
+    A0 = A.clone()
+    w = torch.zeros(n, dtype=torch.float64, device=cuda)
+    V = torch.zeros(n, n, dtype=torch.float64, device=cuda)
+    cv.symm_eig_solve(A, n, w, V, nbw=nbw, nk=512)
+    torch.cuda.synchronize()
+    anorm = float(np.abs(lam).max())
+    dl = float((w.cpu() - torch.from_numpy(np.sort(lam))).abs().max()) / anorm
+    Vl = V.t()                                   # column-major storage -> logical matrix
+    resid = float(torch.linalg.norm(A0 @ Vl - Vl * w[None, :])) / (n * anorm)
+    O_ = Vl.t() @ Vl
+    O_.diagonal().sub_(1.0)
+    orth = float(torch.linalg.norm(O_)) / np.sqrt(n)
+    assert dl < 1e-12, dl
+    assert resid < 1e-13, resid
+    assert orth < 1e-13, orth
+
+
 def test_timer_and_reuse(cuda):
     import cuev_b200 as cv
     A = _sym(600, 3)
