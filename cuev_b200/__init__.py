@@ -85,6 +85,7 @@ _SIGS = {
     "cuev_dsymm_lower": [_VP, _I, _I, _D, _DP, _I, _DP, _I, _D, _DP, _I],
     "cuev_dsyr2k_lower": [_VP, _I, _I, _D, _DP, _I, _DP, _I, _D, _DP, _I],
     "cuev_dsyev_refine": [_DP, _I, _DP, _DP, _I, _D, _VP, C.POINTER(RefineInfo)],
+    "cuev_dsyevd_batched": [_DP, _I, _I, _DP, _DP, _VP],
     "cuev_dsyev_adjoint": [_DP, _DP, _DP, _DP, _I, _D, _DP, _VP],
     "cuev_ssyev_adjoint": [_FP, _FP, _FP, _FP, _I, C.c_float, _FP, _VP],
 }
@@ -206,6 +207,22 @@ def eigvalsh(A_rowmajor_sym, nbw: int = 0, nk: int = 0):
     w = torch.empty(n, dtype=Acm.dtype, device=Acm.device)
     symm_eig_solve(Acm, n, w, None, nbw=nbw, nk=nk)
     return w
+
+
+def eigh_batched(A_batch):
+    """Eigen-decompositions of a stack of small symmetric matrices (batch, n, n), n <= 64, in one
+    launch.  Returns (w, V) with A[b] = V[b] diag(w[b]) V[b]^T; reads the lower triangles."""
+    import torch
+    if A_batch.dim() != 3 or A_batch.shape[1] != A_batch.shape[2]:
+        raise ValueError("expected a (batch, n, n) tensor")
+    bsz, n = A_batch.shape[0], A_batch.shape[1]
+    Acm = A_batch.transpose(1, 2).contiguous()     # column-major storage of each matrix
+    _need_f64(Acm)
+    w = torch.empty(bsz, n, dtype=torch.float64, device=Acm.device)
+    Vcm = torch.empty_like(Acm)
+    _check(lib().cuev_dsyevd_batched(_ptr(Acm), n, bsz, _ptr(w), _ptr(Vcm),
+                                     _stream(None)), "cuev_dsyevd_batched")
+    return w, Vcm.transpose(1, 2)
 
 
 def release_workspace():

@@ -7,6 +7,7 @@
     python -m cuev_b200.bench_kernels refine N [--iters K]       Ogita-Aishima refinement
     python -m cuev_b200.bench_kernels eigvals N                  eigenvalues-only solve
     python -m cuev_b200.bench_kernels adjoint N                  eigh forward + adjoint
+    python -m cuev_b200.bench_kernels batched N BATCH            batched small-n eigh vs torch
 
 `stages` runs the pipeline through the stage entry points (cuev_dbbr_reduce, cuev_bc_chase,
 cuev_tridi_dc, cuev_bc_back, cuev_sbr_back) with an event pair around each, so a profiler can
@@ -234,10 +235,21 @@ def run_adjoint(a):
             "bwd_tflops_6n3": round(6.0 * n ** 3 / b / 1e9, 3)}
 
 
+def run_batched(a):
+    n, bsz = a.M, a.N
+    G = torch.randn(bsz, n, n, dtype=torch.float64, device="cuda",
+                    generator=torch.Generator(device="cuda").manual_seed(3))
+    A = (G + G.transpose(1, 2)) * 0.5
+    ms = _time(lambda: cv.eigh_batched(A), a.reps, a.warmup)
+    ref_ms = _time(lambda: torch.linalg.eigh(A), a.reps, a.warmup)
+    return {"kernel": "eigh_batched", "n": n, "batch": bsz, "ms": round(ms, 3),
+            "torch_linalg_eigh_ms": round(ref_ms, 3)}
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("what", choices=["gemm", "symm", "syr2k", "stages", "refine", "eigvals",
-                                     "adjoint"])
+                                     "adjoint", "batched"])
     ap.add_argument("M", type=int)
     ap.add_argument("N", type=int, nargs="?", default=0)
     ap.add_argument("K", type=int, nargs="?", default=0)
@@ -252,7 +264,8 @@ def main(argv=None):
     if a.what in ("stages", "eigvals", "adjoint") and a.nk == 0:
         a.nk = 512 if a.M >= 8192 else 256
     fn = {"gemm": run_gemm, "symm": run_symm, "syr2k": run_syr2k, "stages": run_stages,
-          "refine": run_refine, "eigvals": run_eigvals, "adjoint": run_adjoint}[a.what]
+          "refine": run_refine, "eigvals": run_eigvals, "adjoint": run_adjoint,
+          "batched": run_batched}[a.what]
     print(json.dumps(fn(a)), flush=True)
 
 

@@ -75,6 +75,15 @@ int cuev_dsyevd_cfg(double *A, int n, double *eval, double *evec, void *stream, 
  * The float input is widened and solved by the FP64 pipeline, then rounded back. */
 int cuev_ssyevd(float *A, int n, float *eval, float *evec, void *stream, cuev_timer *timer);
 
+/* Batched eigensolver for many small matrices (no reference counterpart: the reference solves one
+ * matrix per call).  A holds `batch` symmetric n x n matrices, n <= 64, each column-major and
+ * stored one after another (stride n*n); only their lower triangles are read and A is not
+ * modified.  eval receives batch x n ascending eigenvalues, evec batch x (n x n) eigenvector
+ * columns.  One CTA per matrix (two-sided Jacobi in shared memory).  n > 64 returns
+ * CUEV_ERR_UNSUPPORTED.  Blocks until done. */
+int cuev_dsyevd_batched(const double *A, int n, int batch, double *eval, double *evec,
+                        void *stream);
+
 /* Differentiation form (no reference counterpart): cotangent of A for the eigensolve,
  *   Abar = V (diag(lambar) + sym(F o (V^T Vbar))) V^T,  F_ij = 1/(lam_j - lam_i),
  * sym(X) = (X + X^T)/2, F_ij = 0 on the diagonal and where |lam_j - lam_i| < gap_tol (masked

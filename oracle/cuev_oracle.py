@@ -504,6 +504,16 @@ def tridi_eigvals(d: np.ndarray, e: np.ndarray) -> np.ndarray:
 
 
 # ------------------------------------------------------------------------------------------
+# Batched small-n eigensolver (no reference counterpart): LAPACK per matrix
+# ------------------------------------------------------------------------------------------
+def eigh_batched(A: np.ndarray):
+    """(batch, n, n) symmetric (lower triangles used) -> (w, V), LAPACK dsyevd per matrix."""
+    L = np.tril(A)
+    S = L + np.swapaxes(L, 1, 2) - np.einsum("bii->bi", L)[:, :, None] * np.eye(A.shape[1])
+    return np.linalg.eigh(S)
+
+
+# ------------------------------------------------------------------------------------------
 # Precision form: Ogita-Aishima refinement (no reference counterpart; restates Algorithm 1 of
 # T. Ogita, K. Aishima, Japan J. Indust. Appl. Math. 35 (2018) with the same Frobenius-norm
 # threshold as cuev_b200/csrc/refine.cu)
