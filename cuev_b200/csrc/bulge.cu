@@ -18,7 +18,8 @@
 //    r1, i.e. prog[s-1] >= r1 - b + 1.  That is a two-hop lag instead of the reference's
 //    four (prog >= c + 3b), which halves the pipeline fill.
 //  * per hop the b x 3b strip of the symmetric window that the reflector touches is gathered
-//    into shared memory once, updated there (rank-2 H A H) and written back once.
+//    into shared memory once; each updated element (rank-2 H A H) goes straight back to the band
+//    from the thread that computes it, with no barrier between update and write-back.
 #include "solver.cuh"
 
 #include <algorithm>
@@ -43,7 +44,6 @@ __global__ void __launch_bounds__(BC_THREADS)
     constexpr int NT = BC_THREADS;
     constexpr int NLEFT = (BW * BW + NT - 1) / NT;    // left-block elements per thread
     constexpr int NLOW = (2 * BW * BW + NT - 1) / NT; // lower-part elements per thread
-    constexpr int NUPD = (3 * BW * BW + NT - 1) / NT; // strip elements per thread
     extern __shared__ __align__(16) unsigned char smem_raw[];
     ChaseSmem<BW> &sm = *reinterpret_cast<ChaseSmem<BW> *>(smem_raw);
     const int tid = threadIdx.x;
@@ -154,14 +154,17 @@ __global__ void __launch_bounds__(BC_THREADS)
 
             // ---- p = 2 A w over the window rows
             for (int ii = tid; ii < W; ii += NT) {
-                double a0 = 0.0, a1 = 0.0;
+                // four chains: this dot product is on the hop's critical path
+                double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
                 int k = 0;
-                for (; k + 1 < L; k += 2) {
+                for (; k + 3 < L; k += 4) {
                     a0 = fma(sm.S[k][ii], sm.w[k], a0);
                     a1 = fma(sm.S[k + 1][ii], sm.w[k + 1], a1);
+                    a2 = fma(sm.S[k + 2][ii], sm.w[k + 2], a2);
+                    a3 = fma(sm.S[k + 3][ii], sm.w[k + 3], a3);
                 }
-                if (k < L) a0 = fma(sm.S[k][ii], sm.w[k], a0);
-                sm.p[ii] = 2.0 * (a0 + a1);
+                for (; k < L; ++k) a0 = fma(sm.S[k][ii], sm.w[k], a0);
+                sm.p[ii] = 2.0 * ((a0 + a1) + (a2 + a3));
             }
             __syncthreads();
             // kappa = w^T p over the reflector rows (every warp computes it)
@@ -170,44 +173,41 @@ __global__ void __launch_bounds__(BC_THREADS)
             const double kappa = warp_sum(kl);
             const double beta = sm.red[0];
 
-            // ---- rank-2 update S -= w_row y_col^T + y_row w_col^T with y = p - kappa w;
-            // the reduced column is set exactly: A(r0, cq) = beta, A(r0+1:r1, cq) = 0
-#pragma unroll 4
-            for (int q = 0; q < NUPD; ++q) {
-                const int idx = tid + q * NT;
-                const int ii = idx % (3 * BW), k = idx / (3 * BW);
-                if (ii >= W || k >= L) continue;
-                if (ii == 0) {
-                    sm.S[k][0] = (k == 0) ? beta : 0.0;
-                    continue;
-                }
-                const int kr = ii - off;
-                const double wr = (kr >= 0 && kr < L) ? sm.w[kr] : 0.0;
-                const double wk = sm.w[k];
-                const double yr = sm.p[ii] - kappa * wr;
-                const double yc = sm.p[off + k] - kappa * wk;
-                sm.S[k][ii] -= wr * yc + yr * wk;
-            }
-            __syncthreads();
+            for (int k = tid; k < L; k += NT) U[(r0 + k) + (long long)s * ldu] = sm.w[k];
 
-            // ---- scatter back (left block and lower triangle) and store the reflector
+            // ---- rank-2 update A -= w_row y_col^T + y_row w_col^T with y = p - kappa w, each
+            // element stored to the band straight from the thread that updates it (the strip is
+            // gathered afresh by the next hop, so shared memory keeps the old values); the
+            // reduced column is set exactly: A(r0, cq) = beta, A(r0+1:r1, cq) = 0.
+            // left block (rows above r0, packed column i, contiguous along k)
 #pragma unroll
             for (int q = 0; q < NLEFT; ++q) {
                 const int idx = tid + q * NT;
                 const int k = idx % BW, ii = idx / BW;
-                if (ii < off && k < L) {
-                    const int i = lo + ii, j = r0 + k;
-                    __stcg(&Bp[(j - i) + (long long)i * ldb], sm.S[k][ii]);
+                if (ii >= off || k >= L) continue;
+                double v;
+                if (ii == 0) {
+                    v = (k == 0) ? beta : 0.0;
+                } else { // kr = ii - off < 0: w_row = 0
+                    v = sm.S[k][ii] - sm.p[ii] * sm.w[k];
                 }
+                const int i = lo + ii, j = r0 + k;
+                __stcg(&Bp[(j - i) + (long long)i * ldb], v);
             }
+            // rows r0..hi, lower triangle (packed column j, contiguous along i)
 #pragma unroll
             for (int q = 0; q < NLOW; ++q) {
                 const int idx = tid + q * NT;
                 const int ii = off + idx % (2 * BW), k = idx / (2 * BW);
                 const int i = lo + ii, j = r0 + k;
-                if (ii < W && k < L && i >= j) __stcg(&Bp[(i - j) + (long long)j * ldb], sm.S[k][ii]);
+                if (ii >= W || k >= L || i < j) continue;
+                const int kr = ii - off;
+                const double wr = kr < L ? sm.w[kr] : 0.0;
+                const double wk = sm.w[k];
+                const double yr = sm.p[ii] - kappa * wr;
+                const double yc = sm.p[off + k] - kappa * wk;
+                __stcg(&Bp[(i - j) + (long long)j * ldb], sm.S[k][ii] - (wr * yc + yr * wk));
             }
-            for (int k = tid; k < L; k += NT) U[(r0 + k) + (long long)s * ldu] = sm.w[k];
 
             // ---- publish: the barrier orders every thread's stores before thread 0's release
             // (release is cumulative over what thread 0 has observed through the barrier)
