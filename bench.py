@@ -328,15 +328,19 @@ def run_cuev(args, rank, world, local_rank):
     if tfile.exists():
         try:
             tj = json.loads(tfile.read_text())
-            # DRAM bytes per launch scale with n^2 (M is read and written once per sweep tile)
+            # DRAM bytes per launch grow as n^3: the round-to-round hand-off buffer (n x n) is
+            # written and read once per round of 8 sweep tiles (n / 128 rounds); M itself is
+            # read and written once (n^2).  Scaled from one ncu capture at a smaller n.
             traffic = int(tj["dram_bytes"] * (n / tj["n"]) ** 3)
         except Exception:
             traffic = None
-    roofline = {"kernel": "bc_back_kernel (M <- Q_b M)", "bound": "tensor",
+    roofline = {"kernel": "bc_back_pipe_kernel (M <- Q_b M)", "bound": "tensor",
                 "achieved": round(achieved, 3), "peak": round(fp64_peak, 3), "unit": "TFLOP/s",
                 "frac": round(achieved / fp64_peak, 4), "traffic": traffic,
                 "peak_source": "FP64: cuBLAS DGEMM 8192^3 measured in this run (no FP64 figure "
-                               "in MEASURED_PEAKS.json)",
+                               "in MEASURED_PEAKS.json); the kernel runs on the FP64 FMA pipe, "
+                               "which on this part has the DMMA rate and is shared with it",
+                "algorithmic_bytes_per_launch": int(8 * (2 * n * n + n * n // 2)),
                 "algorithmic_flop_per_launch": bcb_flops}
 
     if rank == 0:
