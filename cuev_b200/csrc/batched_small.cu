@@ -135,8 +135,10 @@ __global__ void __launch_bounds__(BJ_THREADS)
     }
 }
 
-// small per-device status buffer (one word per failure class)
+// small per-device status buffer (one word per failure class); calls are serialised so that one
+// call's reset cannot hide another call's failure
 std::mutex g_bj_mu;
+std::mutex g_bj_call_mu;
 int *g_bj_status[64] = {nullptr};
 
 } // namespace
@@ -153,6 +155,7 @@ int batched_eigh_d(const double *A, int n, int batch, double *eval, double *evec
     int dev = 0;
     CUEV_TRY(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 64) return CUEV_ERR_INVALID;
+    std::lock_guard<std::mutex> call_lock(g_bj_call_mu); // held until the call has synchronised
     int *status = nullptr;
     {
         std::lock_guard<std::mutex> lk(g_bj_mu);

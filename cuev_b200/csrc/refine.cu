@@ -30,6 +30,7 @@ constexpr int RF_THREADS = 256;
 
 // scratch: AX (then I + E), S, G, X_new (n^2 each), partial sums, lam, scalars
 std::mutex g_rf_mu;
+std::mutex g_rf_call_mu; // one refinement at a time: the calls share the scratch below
 void *g_rf_buf[64] = {nullptr};
 size_t g_rf_bytes[64] = {0};
 
@@ -176,6 +177,7 @@ int refine_d(const double *A, int n, double *eval, double *X, int max_iters, dou
     if (!A || !eval || !X) return CUEV_ERR_INVALID;
     const size_t nn = (size_t)n * n;
     const int nblocks = 4 * num_sms();
+    std::lock_guard<std::mutex> call_lock(g_rf_call_mu); // held until the call has synchronised
     void *buf = nullptr;
     CUEV_CHECK_STATUS(rf_scratch(sizeof(double) * (4 * nn + 3 * (size_t)nblocks + n + 8), &buf,
                                  st));

@@ -92,6 +92,8 @@ int cuev_dsyevd_batched(const double *A, int n, int batch, double *eval, double 
  * Enqueued on `stream`, asynchronous. */
 int cuev_dsyev_adjoint(const double *V, const double *lam, const double *Vbar,
                        const double *lambar, int n, double gap_tol, double *Abar, void *stream);
+/* (The adjoint keeps V G in one n x n scratch buffer per device: adjoint calls that can overlap on
+ * the GPU, on different streams, must not share a device.) */
 /* FP32 interface of the same (computed in FP64 internally). */
 int cuev_ssyev_adjoint(const float *V, const float *lam, const float *Vbar, const float *lambar,
                        int n, float gap_tol, float *Abar, void *stream);
@@ -187,6 +189,8 @@ int cuev_back_transform(cuev_handle h, double *evec, cuev_timer *timer);
  * (src/cuda/cublas.cu:15-26). */
 int cuev_dgemm(void *stream, int ta, int tb, int m, int n, int k, double alpha, const double *A,
                int lda, const double *B, int ldb, double beta, double *C, int ldc);
+/* (cuev_dgemm, cuev_dsymm_lower and cuev_dsyr2k_lower keep split-K partial sums in one buffer per
+ * device: calls that can overlap on the GPU, on different streams, must not share a device.) */
 
 /* Same product as cuev_dgemm, for callers that cannot allocate device memory.  No counterpart in
  * the reference.  cuev_dgemm takes its split-K partial-sum buffer from cudaMalloc; a caller whose
