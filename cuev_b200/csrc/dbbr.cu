@@ -205,7 +205,8 @@ __global__ void __launch_bounds__(QR_THREADS)
 // column parity: a CTA overwrites the buffer of column c-1 only after the cluster barrier of
 // column c, which every CTA reaches after its reads of column c-1.
 template <int BW> size_t panel_qr_cluster_smem(int chunk) {
-    return sizeof(double) * ((size_t)chunk * (BW + 1) + BW * BW + 3 * BW + QRC_THREADS + 4 * BW);
+    return sizeof(double) *
+           ((size_t)chunk * (BW + 1) + BW * BW + 3 * BW + QRC_THREADS + 4 * BW + 4);
 }
 
 template <int BW>
@@ -226,6 +227,7 @@ __global__ void __launch_bounds__(QRC_THREADS)
     double *sred = stau + BW;
     double *spart = sred + QRC_THREADS; // [2][BW] this CTA's partial dot products
     double *sroww = spart + 2 * BW;    // [2][BW] row c of the panel (owner CTA only)
+    double *shh = sroww + 2 * BW;      // beta, tau, scale of the current reflector
 
     cg::cluster_group cl = cg::this_cluster();
     const int tid = threadIdx.x;
@@ -270,7 +272,8 @@ __global__ void __launch_bounds__(QRC_THREADS)
         }
         cl.sync();
 
-        // (2) every CTA reduces all partials in the same fixed order (identical results)
+        // (2) every CTA reduces all partials in the same fixed order (identical results); lane c
+        //     of the first row group also forms the reflector's scalars
         {
             double s = 0.0;
             for (int q = rg; q < P; q += NRG) s += cl.map_shared_rank(spart, q)[buf * BW + j];
@@ -280,47 +283,50 @@ __global__ void __launch_bounds__(QRC_THREADS)
                 double tot = 0.0;
 #pragma unroll
                 for (int q = 0; q < NRG; ++q) tot += sred[q * BW + j];
+                const double rowc = cl.map_shared_rank(sroww, c / chunk)[buf * BW + j];
                 sp[j] = tot;
-                srow[j] = cl.map_shared_rank(sroww, c / chunk)[buf * BW + j];
+                srow[j] = rowc;
+                if (j == c) {
+                    // (3) Householder reflector for x = A[c:, c]  (H = I - tau v v^T, v[c] = 1)
+                    const double alpha = rowc, s2 = tot;
+                    double beta = alpha, tauc = 0.0, scal = 0.0;
+                    if (s2 > 0.0) {
+                        beta = -copysign(hypot(alpha, sqrt(s2)), alpha);
+                        tauc = (beta - alpha) / beta;
+                        scal = 1.0 / (alpha - beta);
+                    }
+                    if (!isfinite(s2) || !isfinite(alpha)) dev_fail(status, CUEV_ERR_NONFINITE, c);
+                    shh[0] = beta, shh[1] = tauc, shh[2] = scal;
+                }
             }
             __syncthreads();
         }
+        const double beta = shh[0], tauc = shh[1], scal = shh[2];
 
-        // (3) Householder reflector for x = A[c:, c]  (H = I - tau v v^T, v[c] = 1)
-        const double alpha = srow[c];
-        const double s2 = sp[c];
-        double beta = alpha, tauc = 0.0, scal = 0.0;
-        if (s2 > 0.0) {
-            beta = -copysign(hypot(alpha, sqrt(s2)), alpha);
-            tauc = (beta - alpha) / beta;
-            scal = 1.0 / (alpha - beta);
-        }
-        if (!isfinite(s2) || !isfinite(alpha)) {
-            if (tid == 0) dev_fail(status, CUEV_ERR_NONFINITE, c);
-        }
-        // (4) apply H to the trailing columns of own rows (j > c)
-        if (tauc != 0.0) {
-            if (j > c && j < b) {
-                const double wj = srow[j] + scal * sp[j]; // v^T a_j
-                const double f = tauc * wj;
-#pragma unroll 4
-                for (int r = max(0, c - r0) + rg; r < cnt; r += NRG) {
-                    const int grow = r0 + r;
-                    const double v = (grow == c) ? 1.0 : scal * sP[r * LD + c];
-                    sP[r * LD + j] -= f * v;
-                }
-            }
-        }
-        if (tid < c) sGT[c * BW + tid] = srow[tid] + scal * sp[tid];
-        if (tid == 0) stau[c] = tauc;
-        __syncthreads();
-        // (5) store v_c (scaled) and beta in column c of own rows
+        // (4) store v_c (scaled) and beta in column c of own rows
         for (int r = max(0, c - r0) + tid; r < cnt; r += QRC_THREADS) {
             const int grow = r0 + r;
             if (grow == c)
                 sP[r * LD + c] = beta;
             else if (grow > c)
                 sP[r * LD + c] *= scal;
+        }
+        if (tid < c) sGT[c * BW + tid] = srow[tid] + scal * sp[tid];
+        if (tid == 0) stau[c] = tauc;
+        __syncthreads();
+        // (5) apply H to the trailing columns j > c of own rows, a_j -= tau (v^T a_j) v: the
+        //     (b - 1 - c) columns x own rows spread over all threads, column fastest
+        const int nact = b - 1 - c;
+        if (tauc != 0.0 && nact > 0) {
+            const int groups = QRC_THREADS / nact;
+            if (tid < groups * nact) {
+                const int jj = c + 1 + tid % nact, g0 = tid / nact;
+                const double f = tauc * (srow[jj] + scal * sp[jj]); // tau v^T a_j
+#pragma unroll 4
+                for (int r = max(0, c + 1 - r0) + g0; r < cnt; r += groups)
+                    sP[r * LD + jj] -= f * sP[r * LD + c];
+                if (g0 == 0 && c >= r0 && c < r0 + cnt) sP[(c - r0) * LD + jj] -= f; // v[c] = 1
+            }
         }
         __syncthreads();
     }

@@ -474,17 +474,33 @@ void tile_dims(Tile t, int &bm, int &bn) {
 
 } // namespace
 
-int gemm_splitk_count(int m, int n, int k_total, int c_lower) {
+// Split count from a wave model: with s splits the busiest SM runs ceil(tiles s / SMs) CTAs, each
+// over 1/s of the K range, so the time goes as ceil(tiles s / SMs) / s.  Among the counts that
+// give every SM a CTA (or the largest allowed, when none does), take the smallest one that no
+// larger count beats by 2 % (a split costs a reduction over its m x n partials).  On the band
+// reduction's SYMM (m x 32, K = m) this picks the measured best count to within a few percent for
+// m = 2048 .. 16384, where "at least two CTAs per SM" picked counts up to 1.4x slower.
+int gemm_splitk_count(int m, int n, int k_total, int c_lower, int max_splits) {
     if (m <= 0 || n <= 0 || k_total <= 0) return 1;
     const Tile tl = pick_tile(m, n);
     int bm, bn;
     tile_dims(tl, bm, bn);
     long long tiles = (long long)div_up(m, bm) * div_up(n, bn);
     if (c_lower) tiles = (tiles + div_up(n, bn)) / 2;
-    const int sms = num_sms();
-    if (tiles >= sms) return 1;
-    int s = (int)std::min<long long>((2LL * sms + tiles - 1) / tiles, k_total / 256);
-    return std::max(1, std::min(s, 32));
+    const long long sms = num_sms();
+    if (tiles >= 4 * sms) return 1; // four or more waves: the partial last one costs little
+    // up to 32 splits where 16 cannot fill the SMs, else up to 16 (the range measured)
+    const int scap = tiles * 16 < sms ? 32 : 16;
+    const int smax = std::max(1, std::min({scap, k_total / 256, max_splits}));
+    auto cost = [&](int s) { return (double)((tiles * s + sms - 1) / sms) / s; };
+    int best = 0;
+    double best_t = 0.0;
+    for (int s = 1; s <= smax; ++s) {
+        if (tiles * s < sms && s < smax) continue; // some SMs would idle
+        const double t = cost(s);
+        if (best == 0 || t < 0.98 * best_t) best = s, best_t = t;
+    }
+    return std::max(1, best);
 }
 
 size_t gemm_splitk_workspace(int m, int n, int k_total, int ta, int tb, int c_lower) {

@@ -44,6 +44,7 @@ int gemm_batched_launch(const GemmArgs *dev_args, int count, int max_m, int max_
 
 // Split-K workspace needed by gemm_launch for a problem (0 when no split is used).
 size_t gemm_splitk_workspace(int m, int n, int k_total, int ta, int tb, int c_lower);
-int gemm_splitk_count(int m, int n, int k_total, int c_lower);
+// Split-K count for gemm_launch (at most max_splits, which callers derive from their scratch).
+int gemm_splitk_count(int m, int n, int k_total, int c_lower, int max_splits = 32);
 
 } // namespace cuev

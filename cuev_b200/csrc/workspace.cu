@@ -107,6 +107,12 @@ int workspace_check_status(Workspace *ws, const char *stage) {
     return CUEV_OK;
 }
 
+// splits whose m x n partials fit the workspace's split-K scratch
+static int splitk_fit(const Workspace *ws, int m, int n) {
+    const size_t one = (size_t)m * n * sizeof(double);
+    return one ? (int)std::min<size_t>(32, ws->splitk_bytes / one) : 32;
+}
+
 int ws_gemm2(Workspace *ws, int ta, int tb, int m, int n, int k, int k2, double alpha,
              const double *A, long long lda, const double *A2, long long lda2, const double *B,
              long long ldb, const double *B2, long long ldb2, double beta, double *C,
@@ -116,7 +122,7 @@ int ws_gemm2(Workspace *ws, int ta, int tb, int m, int n, int k, int k2, double 
     a.A = A, a.lda = lda, a.A2 = A2, a.lda2 = lda2;
     a.B = B, a.ldb = ldb, a.B2 = B2, a.ldb2 = ldb2;
     a.C = C, a.ldc = ldc, a.alpha = alpha, a.beta = beta, a.c_lower = c_lower;
-    int splits = gemm_splitk_count(m, n, k + k2, c_lower);
+    int splits = gemm_splitk_count(m, n, k + k2, c_lower, splitk_fit(ws, m, n));
     while (splits > 1 && (size_t)splits * m * n * sizeof(double) > ws->splitk_bytes) --splits;
     a.splits = splits;
     a.ws = splits > 1 ? ws->splitk : nullptr;
@@ -135,7 +141,7 @@ int ws_symm(Workspace *ws, int m, int n, double alpha, const double *A, long lon
     a.m = m, a.n = n, a.k = m;
     a.A = A, a.lda = lda, a.B = B, a.ldb = ldb, a.C = C, a.ldc = ldc;
     a.alpha = alpha, a.beta = beta, a.symm_a = 1;
-    int splits = gemm_splitk_count(m, n, m, 0);
+    int splits = gemm_splitk_count(m, n, m, 0, splitk_fit(ws, m, n));
     while (splits > 1 && (size_t)splits * m * n * sizeof(double) > ws->splitk_bytes) --splits;
     a.splits = splits;
     a.ws = splits > 1 ? ws->splitk : nullptr;
