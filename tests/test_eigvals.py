@@ -24,6 +24,36 @@ def _tridiagonals():
     return out
 
 
+def test_sturm_quotient_method():
+    """The straight-line quotient of the bisection kernel (tridi_eigvals.cu: sturm_quot) restated
+    with exact rounding: a float reciprocal seed off by up to one float ulp (rcp.approx.f32's
+    bound), two Newton steps and Markstein's residual correction land within one rounding of f / q
+    over the pivot range 2^-100 <= |q| <= 2^101 that the kernel's pivot floor guarantees."""
+    from fractions import Fraction as F
+
+    def fma(a, b, c):
+        return float(F(a) * F(b) + F(c))
+
+    rng = np.random.default_rng(11)
+    q_all = rng.uniform(1.0, 2.0, 3000) * 2.0 ** rng.integers(-100, 101, 3000)
+    q_all *= np.where(rng.random(3000) < 0.5, -1.0, 1.0)
+    f_all = rng.random(3000)
+    f_all[:50] = 0.0
+    f_all[50:100] = 1e-310  # subnormal e^2
+    for q, f in zip(q_all.tolist(), f_all.tolist()):
+        q32 = np.float32(q)
+        r32 = np.float32(1.0) / q32
+        exact = F(f) / F(q)
+        for seed in (r32, np.nextafter(r32, np.float32(np.inf)), np.nextafter(r32, np.float32(-np.inf))):
+            r = float(seed)
+            r = fma(r, fma(-q, r, 1.0), r)
+            r = fma(r, fma(-q, r, 1.0), r)
+            y = float(F(f) * F(r))
+            y = fma(r, fma(-q, y, f), y)
+            ulp = float(np.spacing(abs(float(exact)))) if exact != 0 else 0.0
+            assert abs(F(y) - exact) <= F(ulp), (q, f, y, float(exact))
+
+
 def test_oracle_matches_dense():
     rng = np.random.default_rng(3)
     d, e = rng.standard_normal(50), rng.standard_normal(49)
