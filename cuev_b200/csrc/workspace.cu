@@ -9,7 +9,13 @@
 namespace cuev {
 
 namespace {
-size_t splitk_cap_bytes() { return (size_t)3 * num_sms() * 128 * 128 * sizeof(double); }
+// split-K partials: room for two splits of a k x n product (the SBR-back's Y^T M and T X, 512
+// tiles of 128 x 128 at k = 512: 3.5 waves, which split in two run as 7 half-length waves instead
+// of 4 full ones; SBR-back 368 -> 351 ms at n = 16384), and at least three waves' worth of
+// 128 x 128 tiles
+size_t splitk_cap_bytes(size_t n, int k) {
+    return std::max((size_t)3 * num_sms() * 128 * 128, 2 * (size_t)k * n) * sizeof(double);
+}
 } // namespace
 
 int workspace_create(int n, int b, int k, cudaStream_t stream, Workspace **out) {
@@ -31,7 +37,7 @@ int workspace_create(int n, int b, int k, cudaStream_t stream, Workspace **out) 
         size_t bytes;
     };
     ws->qr_part_elems = (size_t)(2 * sms + 2) * 64;
-    ws->splitk_bytes = splitk_cap_bytes();
+    ws->splitk_bytes = splitk_cap_bytes(N, k);
     ws->dc_vec_elems = 24 * N + 64;
     ws->dc_int_elems = 24 * N + 64;
     ws->dc_gemm_args_cap = 2 * (int)(N / 8 + 8);
