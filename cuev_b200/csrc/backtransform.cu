@@ -457,8 +457,14 @@ __global__ void __launch_bounds__(32 * P, 1)
     cp_async_wait<0>(); // leave no copy in flight, also on the early exits
 }
 
-template <int TS, int P> int launch_bc_back_pipe(Workspace *ws, double *M, long long ldm) {
+// Columns [c0, c0 + ncols) of M (c0 a multiple of 32): CTA g owns columns c0 + 32 g .. + 31 and
+// its hand-off rows in dc_S at the offset of its 32-column group, so launches over disjoint
+// column ranges are independent and together do what one launch over all columns does.
+template <int TS, int P>
+int launch_bc_back_pipe(Workspace *ws, cudaStream_t st, double *M, long long ldm, int c0,
+                        int ncols) {
     const int n = ws->n;
+    if (ncols <= 0) return CUEV_OK;
     const size_t smem = sizeof(PipeSmem<TS, P>);
     auto kern = bc_back_pipe_kernel<TS, P>;
     static bool attr = false;
@@ -466,31 +472,20 @@ template <int TS, int P> int launch_bc_back_pipe(Workspace *ws, double *M, long 
         CUEV_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         attr = true;
     }
-    const int grid = div_up(n, 32);
-    kern<<<grid, 32 * P, smem, ws->stream>>>(ws->U, ws->n, M, ldm, ws->dc_S, n, n, ws->status);
+    const int grid = div_up(ncols, 32);
+    double *Xc = ws->dc_S + (size_t)(c0 / 32) * n * 32;
+    kern<<<grid, 32 * P, smem, st>>>(ws->U, ws->n, M + (long long)c0 * ldm, ldm, Xc, n, ncols,
+                                     ws->status);
     note_launch();
     CUEV_TRY(cudaGetLastError());
     return CUEV_OK;
 }
 
-} // namespace
-
-int bc_back(Workspace *ws, double *M, long long ldm) {
-    if (ws->n <= 2) return CUEV_OK;
-    // register window R = TS + b - 1 rows: 79 rows keeps b = 32 spill-free (252 registers);
-    // b = 64 needs the 64 reflector entries live as well and runs a shorter tile
-    if (ws->b == 32) return launch_bc_back_pipe<16, 8>(ws, M, ldm);
-    if (ws->b == 64) return launch_bc_back<64, 16>(ws, M, ldm, ws->n);
-    return CUEV_ERR_INVALID;
-}
-
-int sbr_back(Workspace *ws, double *M, long long ldm) {
+// M <- Q_s M on ncols columns of M, with X (w x ncols) and X2 (w x ncols) as scratch.
+int sbr_back_cols(Workspace *ws, double *M, long long ldm, int ncols, double *X, double *X2) {
     const int n = ws->n, b = ws->b, k = ws->k;
     const long long ld = n;
-    // scratch: X = Y_blk^T M and X2 = T_blk X, both (w x n) with w <= min(k, n), in the D&C
-    // buffers (free once the tridiagonal eigenvectors are formed)
-    double *X = ws->dc_S;
-    double *X2 = ws->dc_Q2;
+    if (ncols <= 0) return CUEV_OK;
     // blocks in reverse order
     int last_i = 0;
     for (int i = 0; i < n; i += k) last_i = i;
@@ -503,11 +498,61 @@ int sbr_back(Workspace *ws, double *M, long long ldm) {
         const double *Yb = ws->Y + (long long)i * ld + (i + b);
         const double *Tb = ws->Tblk + (size_t)(i / k) * k * k;
         double *Mb = M + (i + b);
-        CUEV_CHECK_STATUS(ws_gemm(ws, 1, 0, w, n, rows, 1.0, Yb, ld, Mb, ldm, 0.0, X, w));
-        CUEV_CHECK_STATUS(ws_gemm(ws, 0, 0, w, n, w, 1.0, Tb, k, X, w, 0.0, X2, w));
-        CUEV_CHECK_STATUS(ws_gemm(ws, 0, 0, rows, n, w, -1.0, Yb, ld, X2, w, 1.0, Mb, ldm));
+        CUEV_CHECK_STATUS(ws_gemm(ws, 1, 0, w, ncols, rows, 1.0, Yb, ld, Mb, ldm, 0.0, X, w));
+        CUEV_CHECK_STATUS(ws_gemm(ws, 0, 0, w, ncols, w, 1.0, Tb, k, X, w, 0.0, X2, w));
+        CUEV_CHECK_STATUS(ws_gemm(ws, 0, 0, rows, ncols, w, -1.0, Yb, ld, X2, w, 1.0, Mb, ldm));
     }
     return CUEV_OK;
+}
+
+} // namespace
+
+int bc_back(Workspace *ws, double *M, long long ldm) {
+    if (ws->n <= 2) return CUEV_OK;
+    // register window R = TS + b - 1 rows: 79 rows keeps b = 32 spill-free (252 registers);
+    // b = 64 needs the 64 reflector entries live as well and runs a shorter tile
+    if (ws->b == 32) return launch_bc_back_pipe<16, 8>(ws, ws->stream, M, ldm, 0, ws->n);
+    if (ws->b == 64) return launch_bc_back<64, 16>(ws, M, ldm, ws->n);
+    return CUEV_ERR_INVALID;
+}
+
+int sbr_back(Workspace *ws, double *M, long long ldm) {
+    // scratch: X = Y_blk^T M and X2 = T_blk X, both (w x n) with w <= min(k, n), in the D&C
+    // buffers (free once the tridiagonal eigenvectors are formed)
+    return sbr_back_cols(ws, M, ldm, ws->n, ws->dc_S, ws->dc_Q2);
+}
+
+// Both stages multiply M from the left, so M's columns are independent.  BC-back runs one CTA per
+// 32 columns and one CTA per SM; when its grid ends in a partial wave (n = 16384: 512 CTAs, 3.46
+// waves on 148 SMs) the columns of the whole waves go first, then the last wave runs on the
+// high-priority side stream while the SBR-back of the finished columns fills the idle SMs, and
+// the SBR-back of the last columns follows.  The early SBR-back uses dc_T and dc_Q2 as scratch:
+// the late BC-back's hand-off rows live in dc_S.
+int back_transform(Workspace *ws, double *M, long long ldm, cudaEvent_t bc_end) {
+    const int n = ws->n;
+    const int groups = div_up(std::max(n, 1), 32);
+    const int full = groups / num_sms() * num_sms(); // groups in whole waves
+    if (ws->b != 32 || n <= 2 || full == 0 || full == groups || !ws->side) {
+        CUEV_CHECK_STATUS(bc_back(ws, M, ldm));
+        if (bc_end) CUEV_TRY(cudaEventRecord(bc_end, ws->stream));
+        return sbr_back(ws, M, ldm);
+    }
+    const int c1 = full * 32;
+    CUEV_CHECK_STATUS((launch_bc_back_pipe<16, 8>(ws, ws->stream, M, ldm, 0, c1)));
+    CUEV_TRY(cudaEventRecord(ws->ev_a, ws->stream));
+    CUEV_TRY(cudaStreamWaitEvent(ws->side, ws->ev_a, 0));
+    int st = launch_bc_back_pipe<16, 8>(ws, ws->side, M, ldm, c1, n - c1);
+    if (st == CUEV_OK && bc_end && cudaEventRecord(bc_end, ws->side) != cudaSuccess)
+        st = CUEV_ERR_CUDA;
+    if (st == CUEV_OK && cudaEventRecord(ws->ev_b, ws->side) != cudaSuccess) st = CUEV_ERR_CUDA;
+    if (st == CUEV_OK) st = sbr_back_cols(ws, M, ldm, c1, ws->dc_T, ws->dc_Q2);
+    if (st == CUEV_OK && cudaStreamWaitEvent(ws->stream, ws->ev_b, 0) != cudaSuccess)
+        st = CUEV_ERR_CUDA;
+    if (st != CUEV_OK) {
+        cudaStreamSynchronize(ws->side); // nothing of this call may outlive it on the side stream
+        return st;
+    }
+    return sbr_back_cols(ws, M + (long long)c1 * ldm, ldm, n - c1, ws->dc_T, ws->dc_Q2);
 }
 
 } // namespace cuev

@@ -143,9 +143,8 @@ int solve_d(double *A, int n, double *eval, double *evec, cudaStream_t stream, c
     if (evec) {
         CUEV_CHECK_STATUS(tridi_dc(ws, ws->d, ws->e, eval, evec));
         CUEV_CHECK_STATUS(rec(3));
-        CUEV_CHECK_STATUS(bc_back(ws, evec, n));
-        CUEV_CHECK_STATUS(rec(4));
-        CUEV_CHECK_STATUS(sbr_back(ws, evec, n));
+        // e[4]: BC-back done on every column (its last wave may overlap SBR-back)
+        CUEV_CHECK_STATUS(back_transform(ws, evec, n, timer ? ev.e[4] : nullptr));
     } else { // eigenvalues only: bisection replaces D&C, no back-transform
         CUEV_CHECK_STATUS(tridi_eigvals(ws, ws->d, ws->e, eval));
         CUEV_CHECK_STATUS(rec(3));
@@ -340,9 +339,7 @@ extern "C" int cuev_back_transform(cuev_handle h, double *evec, cuev_timer *time
     EventSet ev;
     if (timer) CUEV_CHECK_STATUS(ev.create());
     if (timer) CUEV_TRY(cudaEventRecord(ev.e[0], ws->stream));
-    CUEV_CHECK_STATUS(bc_back(ws, evec, ws->n));
-    if (timer) CUEV_TRY(cudaEventRecord(ev.e[1], ws->stream));
-    CUEV_CHECK_STATUS(sbr_back(ws, evec, ws->n));
+    CUEV_CHECK_STATUS(back_transform(ws, evec, ws->n, timer ? ev.e[1] : nullptr));
     if (timer) {
         CUEV_TRY(cudaEventRecord(ev.e[2], ws->stream));
         CUEV_TRY(cudaEventSynchronize(ev.e[2]));

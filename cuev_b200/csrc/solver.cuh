@@ -23,6 +23,10 @@ struct Workspace {
     int n = 0, b = 0, k = 0;
     int dev = 0;
     cudaStream_t stream = nullptr;
+    // high-priority stream and two events for the back-transform's overlap of BC-back's last,
+    // partial wave with the SBR-back of the columns already finished
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_a = nullptr, ev_b = nullptr;
 
     double *Y = nullptr, *Z = nullptr, *Wp = nullptr, *Tp = nullptr, *Tblk = nullptr;
     double *tau = nullptr, *Dwk = nullptr, *Cwk = nullptr, *Gblk = nullptr;
@@ -81,5 +85,8 @@ int tridi_eigvals(Workspace *ws, const double *d, const double *e, double *eval)
 // Stage 4: back-transform (backtransform.cu)
 int bc_back(Workspace *ws, double *M, long long ldm);
 int sbr_back(Workspace *ws, double *M, long long ldm);
+// M <- Q_s Q_b M (both stages), overlapped where BC-back's grid ends in a partial wave; records
+// bc_end (when not null) once BC-back has finished every column.
+int back_transform(Workspace *ws, double *M, long long ldm, cudaEvent_t bc_end);
 
 } // namespace cuev

@@ -84,6 +84,16 @@ int workspace_create(int n, int b, int k, cudaStream_t stream, Workspace **out) 
         *it.p = (char *)ws->pool + off;
         off += align256(it.bytes);
     }
+    int least = 0, greatest = 0;
+    if (cudaDeviceGetStreamPriorityRange(&least, &greatest) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&ws->side, cudaStreamNonBlocking, greatest) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ws->ev_a, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ws->ev_b, cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        workspace_destroy(ws);
+        set_last_message("workspace: stream or event creation failed");
+        return CUEV_ERR_CUDA;
+    }
     CUEV_TRY(cudaMemsetAsync(ws->status, 0, DEV_STATUS_WORDS * sizeof(int), stream));
     CUEV_TRY(cudaMemsetAsync(ws->bar, 0, 64, stream));
     *out = ws;
@@ -92,6 +102,9 @@ int workspace_create(int n, int b, int k, cudaStream_t stream, Workspace **out) 
 
 void workspace_destroy(Workspace *ws) {
     if (!ws) return;
+    if (ws->side) cudaStreamSynchronize(ws->side), cudaStreamDestroy(ws->side);
+    if (ws->ev_a) cudaEventDestroy(ws->ev_a);
+    if (ws->ev_b) cudaEventDestroy(ws->ev_b);
     if (ws->pool) cudaFree(ws->pool);
     delete ws;
 }

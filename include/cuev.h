@@ -26,7 +26,7 @@ struct SolveTimer {
     float total_ms = 0;      ///< whole-solve wall clock
     float bt_copyin_ms = 0;  ///< 0: the back-transform works in place on evec
     float bt_qb_ms = 0;      ///< BC-Back  M <- Q_b M
-    float bt_qs_ms = 0;      ///< SBR-Back M <- Q_s M
+    float bt_qs_ms = 0;      ///< SBR-Back M <- Q_s M after BC-back ends (part of it overlaps BC-back)
     float bt_copyout_ms = 0; ///< 0: no copy-out
 };
 

@@ -46,7 +46,8 @@ typedef struct cuev_timer {
     float total_ms;      /* whole-solve wall clock */
     float bt_copyin_ms;  /* kept for layout compatibility (no copy-in is needed here: 0) */
     float bt_qb_ms;      /* BC-Back  M <- Q_b * M */
-    float bt_qs_ms;      /* SBR-Back M <- Q_s * M */
+    float bt_qs_ms;      /* SBR-Back M <- Q_s * M, the part after BC-back ends (SBR-back of the
+                            columns BC-back finished early overlaps its last wave) */
     float bt_copyout_ms; /* kept for layout compatibility (0) */
 } cuev_timer;
 
