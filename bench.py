@@ -3,7 +3,7 @@
 
 One "step" is one full solve of an n x n FP64 matrix A = (G + G^T)/2, G iid N(0, 1) from a seed,
 through cuev_b200 (DBBR -> pack -> bulge chase -> GPU D&C -> back-transform).  The headline
-workload is n = 16384, the size the reference's north-star metric is quoted on; the matrix
+workload is n = 16384, the size the reference's headline throughput is quoted on; the matrix
 (2.1 GB) is far larger than the 126 MB L2, so no flush is needed between steps.
 
 Reported (one JSON line on rank 0):
@@ -11,8 +11,9 @@ Reported (one JSON line on rank 0):
              (work model: DBBR 4/3 n^3 + D&C <= 4/3 n^3 + back-transform 4 n^3)
   e2e        the same metric through the C ABI with HOST buffers: every step copies A from
              pinned host memory, solves, and copies eval + evec back
-  roofline   the bulge-chasing back-transform kernel (one launch, 2 n^3 FLOP) against the FP64
-             peak measured in the same run (cuBLAS DGEMM 8192^3)
+  roofline   the bulge-chasing back-transform kernel (2 n^3 FLOP over its column-range launches,
+             timed from the first start to the last end) against the FP64 peak measured in the
+             same run (cuBLAS DGEMM 8192^3)
   cpu_baseline  the oracle (CPU restatement of the reference pipeline) on a bounded sample
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cuev|reference] [--n N]
