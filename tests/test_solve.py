@@ -115,6 +115,41 @@ def test_config2_full_size(cuda, nbw):
     assert orth < 1e-13, orth
 
 
+@pytest.mark.parametrize("n", [4740, 4768])
+def test_backtransform_overlap_last_group(cuda, n):
+    """The back-transform's BC-back grid at n = 4740 / 4768 is 148 groups of 32 columns (one whole
+    wave on 148 SMs) plus one group 4 / 32 columns wide: the whole wave runs first, then the
+    one-CTA last wave beside the SBR-back of the first 4736 columns, then the SBR-back of the last
+    columns.  Every column must come out right: residual and orthogonality over all of V, and the
+    eigenvalues against the eigenvalues-only path (bisection, no back-transform)."""
+    import torch
+    import cuev_b200 as cv
+    g = torch.Generator(device=cuda).manual_seed(n)
+    G = torch.randn(n, n, dtype=torch.float64, device=cuda, generator=g)
+    A = (G + G.t()) * 0.5                        # symmetric: row- and column-major storage agree
+    del G
+    A0 = A.clone()
+    w_bis = torch.zeros(n, dtype=torch.float64, device=cuda)
+    cv.symm_eig_solve(A0.clone(), n, w_bis, None, nbw=32, nk=256)
+    w = torch.zeros(n, dtype=torch.float64, device=cuda)
+    V = torch.zeros(n, n, dtype=torch.float64, device=cuda)
+    cv.symm_eig_solve(A, n, w, V, nbw=32, nk=256)
+    torch.cuda.synchronize()
+    anorm = float(w_bis.abs().max())
+    dl = float((w - w_bis).abs().max()) / anorm
+    Vl = V.t()                                   # column-major storage -> logical matrix
+    R = A0 @ Vl - Vl * w[None, :]
+    resid = float(torch.linalg.norm(R)) / (n * anorm)
+    worst_col = float(torch.linalg.norm(R, dim=0).max()) / anorm
+    O_ = Vl.t() @ Vl
+    O_.diagonal().sub_(1.0)
+    orth = float(torch.linalg.norm(O_)) / np.sqrt(n)
+    assert dl < 1e-12, dl
+    assert resid < 1e-13, resid
+    assert worst_col < 1e-11, worst_col
+    assert orth < 1e-13, orth
+
+
 def test_timer_and_reuse(cuda):
     import cuev_b200 as cv
     A = _sym(600, 3)
