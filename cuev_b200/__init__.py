@@ -82,6 +82,7 @@ _SIGS = {
     "cuev_back_transform": [_VP, _DP, C.POINTER(Timer)],
     "cuev_dgemm": [_VP, _I, _I, _I, _I, _I, _D, _DP, _I, _DP, _I, _D, _DP, _I],
     "cuev_dgemm_noalloc": [_VP, _I, _I, _I, _I, _I, _D, _DP, _I, _DP, _I, _D, _DP, _I],
+    "cuev_dgemm_i8": [_VP, _I, _I, _I, _I, _I, _I, _D, _DP, _I, _DP, _I, _D, _DP, _I],
     "cuev_dsymm_lower": [_VP, _I, _I, _D, _DP, _I, _DP, _I, _D, _DP, _I],
     "cuev_dsyr2k_lower": [_VP, _I, _I, _D, _DP, _I, _DP, _I, _D, _DP, _I],
     "cuev_dsyev_refine": [_DP, _I, _DP, _DP, _I, _D, _VP, C.POINTER(RefineInfo)],
@@ -330,6 +331,13 @@ def dgemm_noalloc(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, Cm, ldc, stream=
     16 MiB array; m * n <= 1048576; concurrent calls race)."""
     _check(lib().cuev_dgemm_noalloc(_stream(stream), int(ta), int(tb), m, n, k, alpha, _ptr(A),
                                     lda, _ptr(B), ldb, beta, _ptr(Cm), ldc), "cuev_dgemm_noalloc")
+
+
+def dgemm_i8(ta, tb, m, n, k, slices, alpha, A, lda, B, ldb, beta, Cm, ldc, stream=None):
+    """``cuev_dgemm_i8``: the same product emulated on the int8 tensor cores from ``slices``
+    7-bit slices per operand (7: FP64-level, 4: FP32-level accuracy)."""
+    _check(lib().cuev_dgemm_i8(_stream(stream), int(ta), int(tb), m, n, k, int(slices), alpha,
+                               _ptr(A), lda, _ptr(B), ldb, beta, _ptr(Cm), ldc), "cuev_dgemm_i8")
 
 
 def dsymm_lower(m, n, alpha, A, lda, B, ldb, beta, Cm, ldc, stream=None):

@@ -3,6 +3,7 @@
 // a small per-device cache that grows on demand; the solver itself uses its workspace pool.
 #include "common.cuh"
 #include "gemm.cuh"
+#include "tcgemm.cuh"
 
 #include <mutex>
 
@@ -88,4 +89,38 @@ extern "C" int cuev_dsyr2k_lower(void *stream, int n, int k, double alpha, const
     a.B = B, a.ldb = ldb, a.B2 = A, a.ldb2 = lda;
     a.C = C, a.ldc = ldc, a.alpha = alpha, a.beta = beta, a.c_lower = 1;
     return run_gemm(a, 0, 1, (cudaStream_t)stream);
+}
+
+// FP64 GEMM emulated on the int8 tensor cores (tcgemm.cuh): `slices` 7-bit slices per operand
+// (7 gives FP64-level products, 4 FP32-level ones).  Slices and the kernel's status word live in
+// the same per-device scratch as the split-K partials above.  Blocks until the product is done,
+// so that a bounded wait that gave up inside the kernel is returned as CUEV_ERR_TIMEOUT.
+extern "C" int cuev_dgemm_i8(void *stream, int ta, int tb, int m, int n, int k, int slices,
+                             double alpha, const double *A, int lda, const double *B, int ldb,
+                             double beta, double *C, int ldc) {
+    if (m < 0 || n < 0 || k < 0 || !C || (k > 0 && (!A || !B))) return CUEV_ERR_INVALID;
+    if (ldc < m || lda < (ta ? k : m) || ldb < (tb ? n : k)) return CUEV_ERR_INVALID;
+    if (slices < 1 || slices > 8) {
+        set_last_message("cuev_dgemm_i8: slices must be in 1..8");
+        return CUEV_ERR_INVALID;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    if (m == 0 || n == 0) return CUEV_OK;
+    if (k == 0 || alpha == 0.0) return cuev_dgemm(stream, ta, tb, m, n, k, alpha, A, lda, B, ldb,
+                                                  beta, C, ldc);
+    const size_t need = i8_gemm_scratch_bytes(m, n, k, slices) + 256;
+    double *scr = nullptr;
+    CUEV_CHECK_STATUS(scratch_get(need, &scr, st));
+    int *status = (int *)((char *)scr + need - 256);
+    CUEV_TRY(cudaMemsetAsync(status, 0, sizeof(int) * DEV_STATUS_WORDS, st));
+    CUEV_CHECK_STATUS(i8_dgemm(ta, tb, 0, m, n, k, slices, alpha, A, lda, B, ldb, beta, C, ldc, 0,
+                               scr, status, st));
+    int host[DEV_STATUS_WORDS] = {0};
+    CUEV_TRY(cudaMemcpyAsync(host, status, sizeof(host), cudaMemcpyDeviceToHost, st));
+    CUEV_TRY(cudaStreamSynchronize(st));
+    if (host[DEV_STATUS_CODE] != 0) {
+        set_last_message("cuev_dgemm_i8: a bounded wait in the tensor-core kernel gave up");
+        return host[DEV_STATUS_CODE];
+    }
+    return CUEV_OK;
 }
