@@ -15,6 +15,14 @@ Reported (one JSON line on rank 0):
              timed from the first start to the last end) against the FP64 peak measured in the
              same run (cuBLAS DGEMM 8192^3)
   cpu_baseline  the oracle (CPU restatement of the reference pipeline) on a bounded sample
+  stage_roofline  per-stage throughput against the same FP64 peak (DBBR, chase L2 model, D&C
+             upper bound, back-transform) and the whole solve's fraction
+  mixed_refine  the precision form (cuev_dsyevd_mixed) on the same matrix: time, speed-up over
+             the FP64 form, refinement steps and accuracy (outside the headline's timed region)
+  fwd_bwd    forward solve + adjoint (cuev_dsyev_adjoint) at n and at 4096
+The reference arm (--impl reference) runs the reference built from its own sources
+(oracle/_ref/ref_driver) on the same matrix, steps and warm-up where that build and a GPU exist,
+else the oracle port on a bounded CPU sample.
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cuev|reference] [--n N]
 Multi-GPU (replicas only: every rank solves its own matrix; no collective on the data path):
@@ -27,6 +35,7 @@ import json
 import os
 import statistics
 import subprocess
+import tempfile
 import sys
 import time
 from pathlib import Path
@@ -78,10 +87,9 @@ class ClockSampler:
 
     def start(self):
         try:
-            out = ROOT / "gpurun_out"
-            out.mkdir(exist_ok=True)
-            self.path = out / f"clocks_gpu{self.gpu_index}.csv"
-            self.fh = open(self.path, "w")
+            fd, name = tempfile.mkstemp(prefix=f"cuev_clocks_gpu{self.gpu_index}_", suffix=".csv")
+            self.path = Path(name)
+            self.fh = os.fdopen(fd, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
                  "-i", str(self.gpu_index), "-lms", "200"], stdout=self.fh,
@@ -151,13 +159,86 @@ def lapack_dsyevd_sample(n_cpu: int):
     return FLOP_MODEL * n_cpu ** 3 / t / 1e12, t
 
 
+def _bench_matrix(n: int, dev, seed: int):
+    """The bench's input, A = (G + G^T)/2 with G from torch's generator on the device (both arms
+    use the same seed, hence the same matrix)."""
+    import torch
+    g = torch.Generator(device=dev).manual_seed(seed)
+    A0 = torch.randn(n, n, dtype=torch.float64, device=dev, generator=g)
+    return ((A0 + A0.t()) * 0.5).contiguous()
+
+
+def run_reference_driver(args, driver: Path):
+    """The reference's own build (oracle/_ref/ref_driver: the reference's sources compiled
+    unmodified; GPU stages plus its host LAPACK divide and conquer) on the bench's matrix: each
+    step copies A from pinned host memory, calls cuev::symm_eig_solve<double> and copies eval and
+    evec back."""
+    import torch
+    n = args.n
+    dev = torch.device("cuda", 0)
+    A0 = _bench_matrix(n, dev, 1234)
+    shm = Path("/dev/shm")
+    with tempfile.TemporaryDirectory(dir=str(shm) if shm.is_dir() else None) as td:
+        fin = Path(td) / "A.bin"
+        A0.cpu().numpy().tofile(fin)  # symmetric: row-major bytes are its column-major storage
+        del A0
+        torch.cuda.empty_cache()
+        res = subprocess.run([str(driver), str(n), str(fin), "-", "-", str(args.steps),
+                              str(args.warmup)], capture_output=True, text=True,
+                             timeout=60 + 120 * (args.steps + args.warmup))
+    if res.returncode != 0:
+        raise RuntimeError(f"reference driver failed: {res.stderr[-400:]}")
+    recs = [json.loads(x) for x in res.stdout.splitlines() if x.startswith("{")]
+    solve = statistics.median(r["solve_ms"] for r in recs)
+    e2e = statistics.median(r["e2e_ms"] for r in recs)
+    stages = {k: round(statistics.median(r[k] for r in recs), 3)
+              for k in ("dbbr_ms", "bc_ms", "dc_ms", "bt_ms")}
+    return solve, e2e, stages, len(recs)
+
+
 def run_reference(args, rank, world):
-    """The reference arm: the reference pipeline restated on the host cores (the oracle port;
-    the reference itself has no CPU implementation of the path), on a bounded sample."""
+    """The reference arm.  Where the reference built here from its own sources exists
+    (oracle/_ref/ref_driver) and a GPU is present, that build runs the bench's own workload
+    (same n, same matrix, same steps and warm-up).  Otherwise the reference pipeline restated on
+    the host cores (the oracle port) runs a bounded sample."""
     if rank != 0:
         return 0
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    driver = ROOT / "oracle" / "_ref" / "ref_driver"
+    have_gpu = False
+    try:
+        import torch
+        have_gpu = torch.cuda.is_available()
+    except Exception:
+        pass
+    base = {"impl": "reference", "metric": metric_name(args.n), "unit": "TFLOP/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic"}
+    if driver.exists() and have_gpu:
+        n = args.n
+        solve_ms, e2e_ms, stages, cnt = run_reference_driver(args, driver)
+        value = FLOP_MODEL * n ** 3 / (solve_ms * 1e-3) / 1e12
+        line = dict(base)
+        line.update({
+            "value": round(value, 6), "ms_per_step": round(solve_ms, 3),
+            "config": {"workload": f"eigh n={n}: A=(G+G^T)/2, G iid N(0,1), FP64, all "
+                                   "eigenvalues and eigenvectors (the same matrix as the cuev "
+                                   "arm)", "n": n, "nbw": 32, "nk": 512},
+            "stage_ms": stages,
+            "cpu_baseline": {"value": round(value, 6), "unit": "TFLOP/s", "cores": cores,
+                             "kind": "reference",
+                             "sample": f"the reference built from its own sources "
+                                       f"(oracle/_ref/ref_driver) at n={n}, {cnt} timed solves "
+                                       "after the warm-up: its GPU stages plus its host LAPACK "
+                                       f"divide and conquer (OpenMP, up to {cores} host threads)"},
+            "e2e": {"value": round(FLOP_MODEL * n ** 3 / (e2e_ms * 1e-3) / 1e12, 6),
+                    "unit": "TFLOP/s", "h2d_bytes_per_step": 8 * n * n,
+                    "d2h_bytes_per_step": 8 * n * n + 8 * n, "ms_per_step": round(e2e_ms, 3)},
+        })
+        print(json.dumps(line), flush=True)
+        return 0
     n_cpu = args.cpu_n
-    cores = os.cpu_count()
     for _ in range(args.warmup):
         cpu_oracle_sample(n_cpu)
     vals, secs = [], []
@@ -166,11 +247,9 @@ def run_reference(args, rank, world):
         vals.append(v)
         secs.append(t)
     value = statistics.median(vals)
-    line = {
-        "impl": "reference", "metric": metric_name(args.n), "value": round(value, 6),
-        "unit": "TFLOP/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": round(1000 * statistics.median(secs), 3), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+    line = dict(base)
+    line.update({
+        "value": round(value, 6), "ms_per_step": round(1000 * statistics.median(secs), 3),
         "config": {"workload": f"eigh A=(G+G^T)/2, G iid N(0,1); bounded CPU sample n={n_cpu}",
                    "n": args.n, "sample_n": n_cpu},
         "cpu_baseline": {"value": round(value, 6), "unit": "TFLOP/s", "cores": cores,
@@ -180,7 +259,7 @@ def run_reference(args, rank, world):
                                    "bulge chase and LAPACK D&C pieces run sequentially"},
         "e2e": {"value": round(value, 6), "unit": "TFLOP/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
-    }
+    })
     print(json.dumps(line), flush=True)
     return 0
 
@@ -209,10 +288,7 @@ def run_cuev(args, rank, world, local_rank):
     sp = stream.cuda_stream
 
     # input: A = (G + G^T)/2 (symmetric, so column-major storage == row-major storage)
-    g = torch.Generator(device=dev).manual_seed(1234 + rank)
-    A0 = torch.randn(n, n, dtype=torch.float64, device=dev, generator=g)
-    A0 = (A0 + A0.t()) * 0.5
-    A0 = A0.contiguous()
+    A0 = _bench_matrix(n, dev, 1234 + rank)
     A = torch.empty_like(A0)
     w = torch.empty(n, dtype=torch.float64, device=dev)
     V = torch.empty_like(A0)
@@ -320,6 +396,98 @@ def run_cuev(args, rank, world, local_rank):
                "d2h_bytes_per_step": 8 * n * n + 8 * n,
                "ms_per_step": round(tot / steps_e2e, 3)}
 
+    # ---- precision form on the same matrix (outside the headline's timed region)
+    mixed = None
+    if not args.no_mixed:
+        minfo = cv.MixedInfo()
+        mtimer = cv.Timer()
+
+        def solve_mixed():
+            st = lib.cuev_dsyevd_mixed(A.data_ptr(), n, w.data_ptr(), V.data_ptr(), sp,
+                                       C.byref(mtimer), args.mixed_iters, 0.0, C.byref(minfo))
+            if st != 0:
+                raise RuntimeError(f"cuev_dsyevd_mixed failed: {st} "
+                                   f"{lib.cuev_last_error().decode()}")
+
+        w64 = w.clone()  # FP64-form eigenvalues of the same matrix
+        A.copy_(A0)
+        solve_mixed()  # warm-up (allocates the precision form's buffers once)
+        mts, parts = [], []
+        for _ in range(max(1, min(args.steps, 3))):
+            A.copy_(A0)
+            m0, m1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            m0.record(stream)
+            solve_mixed()
+            m1.record(stream)
+            torch.cuda.synchronize()
+            mts.append(m0.elapsed_time(m1))
+            parts.append((minfo.first_ms, minfo.refine_ms))
+        mms = max_over_ranks(statistics.median(mts), dist, dev)
+        with torch.no_grad():
+            Vl = V.t()
+            R = A0 @ Vl - Vl * w[None, :]
+            m_resid = float(torch.linalg.norm(R) / (n * w.abs().max()))
+            del R
+            O_ = Vl.t() @ Vl
+            O_.diagonal().sub_(1.0)
+            m_orth = float(torch.linalg.norm(O_))
+            del O_
+            m_dl = float((w - w64).abs().max() / w64.abs().max())
+            torch.cuda.empty_cache()
+        mixed = {"form": "first solve with the SBR-back GEMMs on FP32-level int8 tensor-core "
+                         f"products, then {args.mixed_iters} Ogita-Aishima step(s) with "
+                         "FP64-level int8 tensor-core products (cuev_dsyevd_mixed)",
+                 "ms_per_step": round(mms, 3),
+                 "value": round(whole_job_tflops(world, 1, n, mms), 4),
+                 "speedup_vs_fp64": round(ms_per / mms, 3),
+                 "first_ms": round(statistics.median(p_[0] for p_ in parts), 2),
+                 "refine_ms": round(statistics.median(p_[1] for p_ in parts), 2),
+                 "refine_iterations": int(minfo.refine_iterations),
+                 "first_stage_ms": {k2: round(getattr(mtimer, k2), 2)
+                                    for k2 in ("dbbr_ms", "bc_ms", "dc_ms", "bt_qb_ms",
+                                               "bt_qs_ms")},
+                 "accuracy": {"resid_n_norm2": m_resid, "orth_fro": m_orth,
+                              "max_dlambda_vs_fp64_rel": m_dl}}
+
+    # ---- differentiation form: forward solve + adjoint (backward), at n and at 4096
+    fwd_bwd = None
+    if not args.no_adjoint:
+        def fb(nn_, A0_):
+            A_ = torch.empty_like(A0_)
+            w_ = torch.empty(nn_, dtype=torch.float64, device=dev)
+            V_ = torch.empty_like(A0_)
+            gw = torch.randn(nn_, dtype=torch.float64, device=dev,
+                             generator=torch.Generator(device=dev).manual_seed(8))
+            gV = torch.randn(nn_, nn_, dtype=torch.float64, device=dev,
+                             generator=torch.Generator(device=dev).manual_seed(9))
+            Ab = torch.empty_like(A0_)
+            fwds, bwds = [], []
+            for r_ in range(3):
+                A_.copy_(A0_)
+                e_ = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+                e_[0].record(stream)
+                st = lib.cuev_dsyevd(A_.data_ptr(), nn_, w_.data_ptr(), V_.data_ptr(), sp, None)
+                e_[1].record(stream)
+                st2 = lib.cuev_dsyev_adjoint(V_.data_ptr(), w_.data_ptr(), gV.data_ptr(),
+                                             gw.data_ptr(), nn_, C.c_double(1e-12),
+                                             Ab.data_ptr(), sp)
+                e_[2].record(stream)
+                torch.cuda.synchronize()
+                if st or st2:
+                    raise RuntimeError(f"fwd/bwd failed: {st} {st2}")
+                if r_ >= 1:
+                    fwds.append(e_[0].elapsed_time(e_[1]))
+                    bwds.append(e_[1].elapsed_time(e_[2]))
+            f_, b_ = statistics.median(fwds), statistics.median(bwds)
+            del A_, V_, gV, Ab
+            torch.cuda.empty_cache()
+            return {"fwd_ms": round(f_, 3), "bwd_ms": round(b_, 3),
+                    "fwd_bwd_ms": round(f_ + b_, 3),
+                    "bwd_tflops": round(6.0 * nn_ ** 3 / (b_ * 1e-3) / 1e12, 3)}
+        fwd_bwd = {str(n): fb(n, A0)}
+        if n != 4096:
+            fwd_bwd["4096"] = fb(4096, _bench_matrix(4096, dev, 4096))
+
     med = {k2: statistics.median(v) for k2, v in stage.items()}
     bcb_ms = med["bt_qb_ms"]
     bcb_flops = 2.0 * n ** 3
@@ -335,7 +503,26 @@ def run_cuev(args, rank, world, local_rank):
             traffic = int(tj["dram_bytes"] * (n / tj["n"]) ** 3)
         except Exception:
             traffic = None
-    roofline = {"kernel": "bc_back_pipe_kernel (M <- Q_b M)", "bound": "tensor",
+    # per-stage figures (algorithmic work / stage time; FP64 peak measured in this run)
+    bq = med["bt_qb_ms"] + med["bt_qs_ms"]
+    stage_rf = {
+        "dbbr": {"tflops": round((4.0 / 3.0) * n ** 3 / (med["dbbr_ms"] * 1e-3) / 1e12, 3)},
+        "bulge_chase": {"l2_gbs_model": round(48.0 * n * n * 32 / (med["bc_ms"] * 1e-3) / 1e9, 1),
+                        "note": "48 n^2 b bytes (the 2b x 3b window read and written per hop), "
+                                "b = 32; latency bound (about 2n + n/b dependent hops)"},
+        "divide_and_conquer": {"tflops_upper": round((4.0 / 3.0) * n ** 3
+                                                     / (med["dc_ms"] * 1e-3) / 1e12, 3),
+                               "note": "4/3 n^3 is the merge GEMMs' flop count without "
+                                       "deflation (an upper bound of the work done)"},
+        "back_transform": {"tflops": round(4.0 * n ** 3 / (bq * 1e-3) / 1e12, 3),
+                           "note": "BC-back 2 n^3 + SBR-back 2 n^3 over BC-back's wall time "
+                                   "plus the SBR-back time after it"},
+    }
+    for v_ in stage_rf.values():
+        if "tflops" in v_:
+            v_["frac"] = round(v_["tflops"] / fp64_peak, 4)
+    stage_rf["whole_solve_frac"] = round(value / world / fp64_peak, 4)
+    roofline = {"kernel": "bc_back_pipe_kernel (M <- Q_b M)", "bound": "fp64_fma",
                 "achieved": round(achieved, 3), "peak": round(fp64_peak, 3), "unit": "TFLOP/s",
                 "frac": round(achieved / fp64_peak, 4), "traffic": traffic,
                 "peak_source": "FP64: cuBLAS DGEMM 8192^3 measured in this run (no FP64 figure "
@@ -372,6 +559,9 @@ def run_cuev(args, rank, world, local_rank):
             "accuracy": {"resid_n_norm2": resid, "resid_fro_rel": resid_ref, "orth_fro": orth},
             "gpu_launches": int(launches),
             "roofline": roofline,
+            "stage_roofline": stage_rf,
+            "mixed_refine": mixed,
+            "fwd_bwd": fwd_bwd,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "clocks": clk,
@@ -395,6 +585,9 @@ def main(argv=None):
     ap.add_argument("--cpu-n", type=int, default=2048)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--mixed-iters", type=int, default=1)
     args = ap.parse_args(argv)
     rank = _env_int("RANK", 0)
     world = _env_int("WORLD_SIZE", 1)

@@ -55,6 +55,21 @@ class Config(C.Structure):
     _fields_ = [("nbw", C.c_int), ("nk", C.c_int)]
 
 
+class MixedInfo(C.Structure):
+    """cuev_mixed_info: refinement steps, last measured norms and the two parts' times."""
+
+    _fields_ = [("refine_iterations", C.c_int), ("offdiag_fro", C.c_double),
+                ("orth_fro", C.c_double), ("anorm", C.c_double), ("first_ms", C.c_float),
+                ("refine_ms", C.c_float)]
+
+    def as_dict(self):
+        return {n: (float(getattr(self, n)) if n != "refine_iterations"
+                    else int(getattr(self, n))) for n, _ in self._fields_}
+
+
+PRODUCTS_FP64, PRODUCTS_INT8 = 0, 1
+
+
 class RefineInfo(C.Structure):
     """cuev_refine_info: steps applied and the norms measured on the last X."""
 
@@ -86,7 +101,11 @@ _SIGS = {
     "cuev_dsymm_lower": [_VP, _I, _I, _D, _DP, _I, _DP, _I, _D, _DP, _I],
     "cuev_dsyr2k_lower": [_VP, _I, _I, _D, _DP, _I, _DP, _I, _D, _DP, _I],
     "cuev_dsyev_refine": [_DP, _I, _DP, _DP, _I, _D, _VP, C.POINTER(RefineInfo)],
+    "cuev_dsyev_refine_ex": [_DP, _I, _DP, _DP, _I, _D, _I, _VP, C.POINTER(RefineInfo)],
+    "cuev_dsyevd_mixed": [_DP, _I, _DP, _DP, _VP, C.POINTER(Timer), _I, _D,
+                          C.POINTER(MixedInfo)],
     "cuev_dsyevd_batched": [_DP, _I, _I, _DP, _DP, _VP],
+    "cuev_debug_set_wait_limit_ns": [C.c_ulonglong],
     "cuev_dsyev_adjoint": [_DP, _DP, _DP, _DP, _I, _D, _DP, _VP],
     "cuev_ssyev_adjoint": [_FP, _FP, _FP, _FP, _I, C.c_float, _FP, _VP],
 }
@@ -187,15 +206,34 @@ def eigh(A_rowmajor_sym, nbw: int = 0, nk: int = 0):
 
 
 def refine(A, n: int, eval, evec, max_iters: int = 2, tol: float = 0.0,
-           stream=None) -> RefineInfo:
+           stream=None, products: int = PRODUCTS_FP64) -> RefineInfo:
     """Ogita-Aishima refinement in place: ``evec`` (column-major n x n eigenvector columns) is
     improved against the symmetric ``A`` (column-major, lower triangle read, not modified) and
-    ``eval`` receives the refined eigenvalues.  Returns the step count and measured norms."""
+    ``eval`` receives the refined eigenvalues.  ``products``: PRODUCTS_FP64 (DMMA) or
+    PRODUCTS_INT8 (int8 tensor cores).  Returns the step count and measured norms."""
     _need_f64(A, eval, evec)
     info = RefineInfo()
-    st = lib().cuev_dsyev_refine(_ptr(A), n, _ptr(eval), _ptr(evec), max_iters, tol,
-                                 _stream(stream), C.byref(info))
+    if products == PRODUCTS_FP64:
+        st = lib().cuev_dsyev_refine(_ptr(A), n, _ptr(eval), _ptr(evec), max_iters, tol,
+                                     _stream(stream), C.byref(info))
+    else:
+        st = lib().cuev_dsyev_refine_ex(_ptr(A), n, _ptr(eval), _ptr(evec), max_iters, tol,
+                                        int(products), _stream(stream), C.byref(info))
     _check(st, "cuev_dsyev_refine")
+    return info
+
+
+def symm_eig_solve_mixed(A, n: int, eval, evec, max_refine_iters: int = 2, tol: float = 0.0,
+                         stream=None, timer: Timer | None = None) -> MixedInfo:
+    """Precision form (``cuev_dsyevd_mixed``): same arguments and result as ``symm_eig_solve``
+    (FP64 tensors, A overwritten); FP32-level tensor-core first solve, then refinement with
+    FP64-level int8 tensor-core products.  Returns the refinement record."""
+    _need_f64(A, eval, evec)
+    info = MixedInfo()
+    t = C.byref(timer) if timer is not None else None
+    st = lib().cuev_dsyevd_mixed(_ptr(A), n, _ptr(eval), _ptr(evec), _stream(stream), t,
+                                 int(max_refine_iters), float(tol), C.byref(info))
+    _check(st, "cuev_dsyevd_mixed")
     return info
 
 
@@ -226,6 +264,12 @@ def eigh_batched(A_batch):
     return w, Vcm.transpose(1, 2)
 
 
+def debug_set_wait_limit_ns(ns: int) -> None:
+    """Failure-path tests only: every bounded device wait gives up after `ns` nanoseconds
+    (0 restores the default 2 s)."""
+    _check(lib().cuev_debug_set_wait_limit_ns(int(ns)), "cuev_debug_set_wait_limit_ns")
+
+
 def release_workspace():
     _check(lib().cuev_release_workspace(), "cuev_release_workspace")
 
@@ -234,20 +278,36 @@ def release_workspace():
 # Stage-level API (reference SolverHandle<T> + cuev::kernels::*)
 # ------------------------------------------------------------------------------------------
 class SolverHandle:
-    """Mirror of the reference ``SolverHandle<double>`` (handle_alloc / handle_free)."""
+    """Mirror of the reference ``SolverHandle<double>`` (handle_alloc / handle_free).
+
+    ``buffer()`` returns torch views of the handle's device buffers.  The workspace is released
+    only once the handle is closed AND every such view is gone, so a view that outlives the
+    ``with`` block (a traceback that prints it, say) never reads freed device memory."""
 
     def __init__(self, n: int, nbw: int = 32, nk: int = 512, stream=None):
         self.n, self.nbw, self.nk = n, nbw, nk
         self._stream = _stream(stream)
+        self._views = 0
+        self._closed = False
         h = C.c_void_p()
         _check(lib().cuev_handle_create(n, nbw, nk, self._stream, C.byref(h)),
                "cuev_handle_create")
         self.h = h
 
-    def close(self):
+    def _destroy(self):
         if getattr(self, "h", None):
-            _check(lib().cuev_handle_destroy(self.h), "cuev_handle_destroy")
-            self.h = None
+            h, self.h = self.h, None
+            _check(lib().cuev_handle_destroy(h), "cuev_handle_destroy")
+
+    def _view_gone(self):
+        self._views -= 1
+        if self._closed and self._views == 0:
+            self._destroy()
+
+    def close(self):
+        self._closed = True
+        if getattr(self, "_views", 0) == 0:
+            self._destroy()
 
     def __enter__(self):
         return self
@@ -257,7 +317,8 @@ class SolverHandle:
 
     def __del__(self):
         try:
-            self.close()
+            self._closed = True
+            self._destroy()
         except Exception:
             pass
 
@@ -265,11 +326,18 @@ class SolverHandle:
         """A torch view (column-major storage as a (cols, ld) row-major tensor) of a handle
         buffer; returns (tensor, ld)."""
         import torch
+        import weakref
         p = C.c_void_p()
         ld = C.c_longlong()
         _check(lib().cuev_handle_buffer(self.h, which, C.byref(p), C.byref(ld)),
                "cuev_handle_buffer")
-        return _wrap_device(p.value, cols * ld.value, torch.float64).view(cols, ld.value), ld.value
+        t, holder = _wrap_device(p.value, cols * ld.value, torch.float64, with_holder=True)
+        # the tensor's storage keeps `holder` alive; when the last tensor sharing it is gone the
+        # holder is collected and the handle may free its workspace
+        self._views += 1
+        fin = weakref.finalize(holder, self._view_gone)
+        fin.atexit = False  # at interpreter exit the process releases the device memory anyway
+        return t.view(cols, ld.value), ld.value
 
     # stage launchers -----------------------------------------------------------------------
     def dbbr_panel_qr(self, A, lda, Y, ldy, tau, T, rows, b):
@@ -303,8 +371,9 @@ class SolverHandle:
         _check(lib().cuev_back_transform(self.h, _ptr(evec), t), "back_transform")
 
 
-def _wrap_device(ptr: int, numel: int, dtype):
-    """Non-owning torch view of device memory owned by the library."""
+def _wrap_device(ptr: int, numel: int, dtype, with_holder: bool = False):
+    """Non-owning torch view of device memory owned by the library (torch keeps a reference to
+    the interface object for as long as the tensor's storage lives)."""
     import torch
 
     class _Holder:
@@ -315,7 +384,8 @@ def _wrap_device(ptr: int, numel: int, dtype):
         "shape": (numel,), "typestr": "<f8" if dtype == torch.float64 else "<f4",
         "data": (ptr, False), "version": 2, "strides": None,
     }
-    return torch.as_tensor(h, device="cuda")
+    t = torch.as_tensor(h, device="cuda")
+    return (t, h) if with_holder else t
 
 
 # ------------------------------------------------------------------------------------------

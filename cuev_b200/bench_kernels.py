@@ -1,11 +1,13 @@
 """Per-kernel timings of libcuev_b200 through its C ABI (CUDA events on the launching stream).
 
     python -m cuev_b200.bench_kernels gemm M N K [--ta] [--tb]   DMMA GEMM vs torch (cuBLAS)
+    python -m cuev_b200.bench_kernels i8gemm M N K [--slices S]  FP64 GEMM emulated on int8 tcgen05
     python -m cuev_b200.bench_kernels symm M N                   C = A B, A symmetric (lower)
     python -m cuev_b200.bench_kernels syr2k N K                  lower(C) = A B^T + B A^T
     python -m cuev_b200.bench_kernels stages N                   every solver stage on its own
     python -m cuev_b200.bench_kernels refine N [--iters K]       Ogita-Aishima refinement
     python -m cuev_b200.bench_kernels eigvals N                  eigenvalues-only solve
+    python -m cuev_b200.bench_kernels mixed N [--iters K]        precision form vs FP64 solve
     python -m cuev_b200.bench_kernels adjoint N                  eigh forward + adjoint
     python -m cuev_b200.bench_kernels batched N BATCH            batched small-n eigh vs torch
 
@@ -65,6 +67,23 @@ def run_gemm(a):
     return {"kernel": "dgemm", "m": m, "n": n, "k": k, "ta": a.ta, "tb": a.tb,
             "ms": round(ms, 4), "tflops": round(fl / ms / 1e9, 3),
             "cublas_ms": round(ref_ms, 4), "cublas_tflops": round(fl / ref_ms / 1e9, 3)}
+
+
+def run_i8gemm(a):
+    """cuev_dgemm_i8 (slicing + tcgen05 int8 products, one call); int8 TOPS count
+    s (s + 1) / 2 slice products of 2 m n k operations each."""
+    m, n, k, s = a.M, a.N, a.K, a.slices
+    A = _rand(k, m, 1)
+    B = _rand(n, k, 2)
+    Cm = torch.zeros(n, m, dtype=torch.float64, device="cuda")
+    ms = _time(lambda: cv.dgemm_i8(0, 0, m, n, k, s, 1.0, A, m, B, k, 0.0, Cm, m),
+               a.reps, a.warmup)
+    ref_ms = _time(lambda: torch.matmul(A.t(), B.t()), a.reps, a.warmup)
+    fl = 2.0 * m * n * k
+    ops = fl * s * (s + 1) / 2
+    return {"kernel": "dgemm_i8", "m": m, "n": n, "k": k, "slices": s, "ms": round(ms, 4),
+            "fp64_equiv_tflops": round(fl / ms / 1e9, 3), "int8_tops": round(ops / ms / 1e9, 1),
+            "cublas_dgemm_ms": round(ref_ms, 4), "cublas_tflops": round(fl / ref_ms / 1e9, 3)}
 
 
 def run_symm(a):
@@ -172,6 +191,58 @@ def run_refine(a):
     return out
 
 
+def _metrics_gpu(A, w, Vcm):
+    """Residual ||A V - V diag(w)||_F / (n ||A||_2), orthogonality ||V^T V - I||_F (FP64 on the
+    GPU; ||A||_2 = max |w|)."""
+    n = A.shape[0]
+    V = Vcm.view(n, n).t()
+    R = A @ V - V * w[None, :]
+    an = w.abs().max()
+    I = torch.eye(n, dtype=torch.float64, device="cuda")
+    return {"resid_n_norm2": float(torch.linalg.norm(R) / (n * an)),
+            "orth_fro": float(torch.linalg.norm(V.t() @ V - I))}
+
+
+def run_mixed(a):
+    """The same seeded matrix through cuev_dsyevd (FP64) and cuev_dsyevd_mixed (FP32-level int8
+    tensor-core first solve + --iters refinement steps); solve times by CUDA events."""
+    n = a.M
+    G = _rand(n, n, 7)
+    A = (G + G.t()) / 2
+    del G
+    st = torch.cuda.current_stream()
+    out = {"n": n, "refine_iters": a.iters}
+    for form in ("fp64", "mixed"):
+        ts = []
+        for r in range(a.warmup + a.reps):
+            Acm = A.clone()  # symmetric: its storage is its column-major storage
+            w = torch.empty(n, dtype=torch.float64, device="cuda")
+            V = torch.empty(n * n, dtype=torch.float64, device="cuda")
+            tm = cv.Timer()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(st)
+            if form == "fp64":
+                cv.symm_eig_solve(Acm, n, w, V, timer=tm)
+                info = None
+            else:
+                info = cv.symm_eig_solve_mixed(Acm, n, w, V, max_refine_iters=a.iters, timer=tm)
+            e1.record(st)
+            torch.cuda.synchronize()
+            if r >= a.warmup:
+                ts.append(e0.elapsed_time(e1))
+            del Acm
+        rec = {"ms": round(statistics.median(ts), 2), "stages": tm.as_dict()}
+        if info is not None:
+            rec["refine"] = info.as_dict()
+        rec.update(_metrics_gpu(A, w, V))
+        out[form] = rec
+        del V
+        torch.cuda.empty_cache()
+    out["speedup_mixed_vs_fp64"] = round(out["fp64"]["ms"] / out["mixed"]["ms"], 3)
+    return out
+
+
 def run_eigvals(a):
     """Eigenvalues-only solve (evec = NULL) through the C ABI, with the per-stage timer."""
     n = a.M
@@ -248,8 +319,8 @@ def run_batched(a):
 
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
-    ap.add_argument("what", choices=["gemm", "symm", "syr2k", "stages", "refine", "eigvals",
-                                     "adjoint", "batched"])
+    ap.add_argument("what", choices=["gemm", "i8gemm", "symm", "syr2k", "stages", "refine",
+                                     "eigvals", "adjoint", "batched", "mixed"])
     ap.add_argument("M", type=int)
     ap.add_argument("N", type=int, nargs="?", default=0)
     ap.add_argument("K", type=int, nargs="?", default=0)
@@ -258,14 +329,15 @@ def main(argv=None):
     ap.add_argument("--nbw", type=int, default=32)
     ap.add_argument("--nk", type=int, default=0)
     ap.add_argument("--iters", type=int, default=2)
+    ap.add_argument("--slices", type=int, default=7)
     ap.add_argument("--reps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=2)
     a = ap.parse_args(argv)
     if a.what in ("stages", "eigvals", "adjoint") and a.nk == 0:
         a.nk = 512 if a.M >= 8192 else 256
-    fn = {"gemm": run_gemm, "symm": run_symm, "syr2k": run_syr2k, "stages": run_stages,
+    fn = {"gemm": run_gemm, "i8gemm": run_i8gemm, "symm": run_symm, "syr2k": run_syr2k, "stages": run_stages,
           "refine": run_refine, "eigvals": run_eigvals, "adjoint": run_adjoint,
-          "batched": run_batched}[a.what]
+          "batched": run_batched, "mixed": run_mixed}[a.what]
     print(json.dumps(fn(a)), flush=True)
 
 

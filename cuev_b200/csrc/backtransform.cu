@@ -184,11 +184,7 @@ template <int BW, int TS> int launch_bc_back(Workspace *ws, double *M, long long
     constexpr int NT = 32 * NWARP;
     const size_t smem = bc_back_smem<BW, TS>(NT);
     auto kern = bc_back_kernel<BW, TS, NWARP>;
-    static bool attr = false;
-    if (!attr) {
-        CUEV_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr = true;
-    }
+    CUEV_CHECK_STATUS(ensure_dyn_smem((const void *)kern, smem));
     const int grid = div_up(ncols, NT);
     kern<<<grid, NT, smem, ws->stream>>>(ws->U, ws->n, M, ldm, ws->n, ncols); note_launch();
     CUEV_TRY(cudaGetLastError());
@@ -259,7 +255,7 @@ __device__ __forceinline__ bool pipe_wait(const int *flag, int target, int *abor
         __nanosleep(32);
         if (lds_acquire(flag) >= target) return true;
         if (*(volatile int *)abort_flag) return false;
-        if (global_ns() - t0 > 2000000000ull) {
+        if (global_ns() - t0 > wait_limit_ns(status)) {
             dev_fail(status, CUEV_ERR_TIMEOUT, where);
             *(volatile int *)abort_flag = 1;
             return false;
@@ -467,11 +463,7 @@ int launch_bc_back_pipe(Workspace *ws, cudaStream_t st, double *M, long long ldm
     if (ncols <= 0) return CUEV_OK;
     const size_t smem = sizeof(PipeSmem<TS, P>);
     auto kern = bc_back_pipe_kernel<TS, P>;
-    static bool attr = false;
-    if (!attr) {
-        CUEV_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr = true;
-    }
+    CUEV_CHECK_STATUS(ensure_dyn_smem((const void *)kern, smem));
     const int grid = div_up(ncols, 32);
     double *Xc = ws->dc_S + (size_t)(c0 / 32) * n * 32;
     kern<<<grid, 32 * P, smem, st>>>(ws->U, ws->n, M + (long long)c0 * ldm, ldm, Xc, n, ncols,
@@ -479,6 +471,18 @@ int launch_bc_back_pipe(Workspace *ws, cudaStream_t st, double *M, long long ldm
     note_launch();
     CUEV_TRY(cudaGetLastError());
     return CUEV_OK;
+}
+
+// One SBR-back product.  In the precision form (ws->mixed) products of at least 2^30
+// multiply-adds run on the int8 tensor cores at FP32-level accuracy (MIXED_SLICES slices);
+// smaller ones cost more in slicing than they save.
+int bt_gemm(Workspace *ws, int ta, int tb, int m, int n, int k, double alpha, const double *A,
+            long long lda, const double *B, long long ldb, double beta, double *C, long long ldc) {
+    if (ws->mixed && alpha != 0.0 && (double)m * n * k >= 1073741824.0 &&
+        i8_gemm_scratch_bytes(m, n, k, MIXED_SLICES) <= ws->i8_scratch_bytes)
+        return i8_dgemm(ta, tb, 0, m, n, k, MIXED_SLICES, alpha, A, lda, B, ldb, beta, C, ldc, 0,
+                        ws->i8_scratch, ws->status, ws->stream);
+    return ws_gemm(ws, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
 }
 
 // M <- Q_s M on ncols columns of M, with X (w x ncols) and X2 (w x ncols) as scratch.
@@ -498,9 +502,9 @@ int sbr_back_cols(Workspace *ws, double *M, long long ldm, int ncols, double *X,
         const double *Yb = ws->Y + (long long)i * ld + (i + b);
         const double *Tb = ws->Tblk + (size_t)(i / k) * k * k;
         double *Mb = M + (i + b);
-        CUEV_CHECK_STATUS(ws_gemm(ws, 1, 0, w, ncols, rows, 1.0, Yb, ld, Mb, ldm, 0.0, X, w));
-        CUEV_CHECK_STATUS(ws_gemm(ws, 0, 0, w, ncols, w, 1.0, Tb, k, X, w, 0.0, X2, w));
-        CUEV_CHECK_STATUS(ws_gemm(ws, 0, 0, rows, ncols, w, -1.0, Yb, ld, X2, w, 1.0, Mb, ldm));
+        CUEV_CHECK_STATUS(bt_gemm(ws, 1, 0, w, ncols, rows, 1.0, Yb, ld, Mb, ldm, 0.0, X, w));
+        CUEV_CHECK_STATUS(bt_gemm(ws, 0, 0, w, ncols, w, 1.0, Tb, k, X, w, 0.0, X2, w));
+        CUEV_CHECK_STATUS(bt_gemm(ws, 0, 0, rows, ncols, w, -1.0, Yb, ld, X2, w, 1.0, Mb, ldm));
     }
     return CUEV_OK;
 }
@@ -549,7 +553,11 @@ int back_transform(Workspace *ws, double *M, long long ldm, cudaEvent_t bc_end) 
     if (st == CUEV_OK && cudaStreamWaitEvent(ws->stream, ws->ev_b, 0) != cudaSuccess)
         st = CUEV_ERR_CUDA;
     if (st != CUEV_OK) {
-        cudaStreamSynchronize(ws->side); // nothing of this call may outlive it on the side stream
+        // nothing of this call may outlive it on the side stream: join the side stream back into
+        // the caller's stream (an event, not a host synchronisation, which would be illegal while
+        // the caller's stream is being captured)
+        if (cudaEventRecord(ws->ev_b, ws->side) == cudaSuccess)
+            cudaStreamWaitEvent(ws->stream, ws->ev_b, 0);
         return st;
     }
     return sbr_back_cols(ws, M + (long long)c1 * ldm, ldm, n - c1, ws->dc_T, ws->dc_Q2);

@@ -164,13 +164,8 @@ int batched_eigh_d(const double *A, int n, int batch, double *eval, double *evec
     }
     const int m = n + (n & 1);
     const size_t smem = sizeof(double) * 2 * (size_t)m * (m + 1);
-    static bool attr = false;
-    if (!attr) {
-        CUEV_TRY(cudaFuncSetAttribute(batched_jacobi_kernel,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)(sizeof(double) * 2 * BJ_MAXN * (BJ_MAXN + 1))));
-        attr = true;
-    }
+    CUEV_CHECK_STATUS(ensure_dyn_smem((const void *)batched_jacobi_kernel,
+                                      sizeof(double) * 2 * BJ_MAXN * (BJ_MAXN + 1)));
     CUEV_TRY(cudaMemsetAsync(status, 0, DEV_STATUS_WORDS * sizeof(int), st));
     batched_jacobi_kernel<<<batch, BJ_THREADS, smem, st>>>(A, n, eval, evec, status);
     note_launch();

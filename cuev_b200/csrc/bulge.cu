@@ -73,10 +73,13 @@ __global__ void __launch_bounds__(BC_THREADS)
                 if (s > 0) {
                     const int need = r1 - b + 1;
                     const uint64_t t0 = global_ns();
+                    const uint64_t limit = wait_limit_ns(status);
+                    // the clock is read every 256 polls, or every poll under a short limit
+                    const int every = limit < 1000000ull ? 0 : 255;
                     int spins = 0;
                     while (ld_acquire(&prog[s - 1]) < need) {
-                        if ((++spins & 255) == 0) {
-                            if (global_ns() - t0 > 2000000000ull ||
+                        if ((++spins & every) == 0) {
+                            if (global_ns() - t0 > limit ||
                                 ld_acquire(&status[DEV_STATUS_CODE]) != 0) {
                                 dev_fail(status, CUEV_ERR_TIMEOUT, s);
                                 ok = 0;
@@ -236,11 +239,7 @@ template <int BW> int launch_chase(Workspace *ws, double *B) {
     const int nsweeps = n - 2;
     const size_t smem = sizeof(ChaseSmem<BW>);
     auto kern = bc_chase_kernel<BW>;
-    static bool attr = false;
-    if (!attr) {
-        CUEV_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr = true;
-    }
+    CUEV_CHECK_STATUS(ensure_dyn_smem((const void *)kern, smem));
     int per_sm = 0;
     CUEV_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, BC_THREADS, smem));
     const int cap = std::max(1, per_sm) * num_sms();

@@ -3,6 +3,7 @@
 // Full solves keep one cached workspace per device and (n, b, k) so repeated calls do not
 // allocate; a call that finds the cached workspace busy (another host thread) allocates its own,
 // which keeps the reference's reentrancy (its handle is per call, src/cuda/solver.cu:33,72).
+#include "refine.cuh"
 #include "solver.cuh"
 
 #include "../../include/cuev.h"
@@ -42,8 +43,9 @@ int acquire_ws(int n, int b, int k, cudaStream_t stream, Workspace **out, bool *
         std::lock_guard<std::mutex> lk(g_cache_mu);
         CachedWs &c = g_cache[dev & 63];
         if (!c.busy) {
+            // a cached workspace that is not busy has no work in flight (solves block until
+            // done); workspace_destroy waits for its own side stream
             if (c.ws && (c.ws->n != n || c.ws->b != b || c.ws->k != k)) {
-                cudaDeviceSynchronize();
                 workspace_destroy(c.ws);
                 c.ws = nullptr;
             }
@@ -101,11 +103,28 @@ struct EventSet {
     }
 };
 
+// Clears the workspace's precision-form flag on every exit path.
+struct MixedFlag {
+    Workspace *ws;
+    ~MixedFlag() {
+        if (ws) ws->mixed = 0;
+    }
+};
+
+// mixed == nullptr: the plain FP64 solve.  Otherwise the precision form: A's FP64-level slices
+// are taken first, the solve runs with ws->mixed set, then the eigenpairs are refined.
+struct MixedReq {
+    int max_iters;
+    double tol;
+    cuev_mixed_info *info;
+};
+
 int solve_d(double *A, int n, double *eval, double *evec, cudaStream_t stream, cuev_timer *timer,
-            const cuev_config *cfg) {
+            const cuev_config *cfg, const MixedReq *mixed = nullptr) {
     if (n < 0) return CUEV_ERR_INVALID;
     if (n == 0) return CUEV_OK;
     if (!A || !eval) return CUEV_ERR_INVALID; // evec == NULL: eigenvalues only
+    if (mixed && !evec) return CUEV_ERR_INVALID;
     auto wall0 = std::chrono::high_resolution_clock::now();
     if (n == 1) {
         small_solve_kernel<<<1, 1, 0, stream>>>(A, eval, evec); note_launch();
@@ -131,10 +150,19 @@ int solve_d(double *A, int n, double *eval, double *evec, cudaStream_t stream, c
         if (timer) CUEV_TRY(cudaEventRecord(ev.e[i], stream));
         return CUEV_OK;
     };
+    CUEV_CHECK_STATUS(apply_wait_limit(ws->status, stream));
     nonfinite_scan_kernel<<<4 * num_sms(), 256, 0, stream>>>(A, n, n, ws->status); note_launch();
     CUEV_TRY(cudaGetLastError());
     CUEV_CHECK_STATUS(workspace_check_status(ws, "input scan"));
 
+    MixedFlag mflag{nullptr};
+    if (mixed) {
+        CUEV_CHECK_STATUS(workspace_enable_mixed(ws));
+        // the refinement measures against the original A: keep it as FP64-level slices
+        CUEV_CHECK_STATUS(i8_slice(A, n, I8_SRC_SYML, ws->a_sl, stream));
+        ws->mixed = 1;
+        mflag.ws = ws;
+    }
     CUEV_CHECK_STATUS(rec(0));
     CUEV_CHECK_STATUS(dbbr_reduce(ws, A));
     CUEV_CHECK_STATUS(rec(1));
@@ -153,6 +181,22 @@ int solve_d(double *A, int n, double *eval, double *evec, cudaStream_t stream, c
     CUEV_CHECK_STATUS(rec(5));
     CUEV_CHECK_STATUS(workspace_check_status(ws, "solve"));
     auto wall1 = std::chrono::high_resolution_clock::now();
+    if (mixed) {
+        ws->mixed = 0;
+        cuev_refine_info ri{};
+        CUEV_CHECK_STATUS(refine_core(nullptr, &ws->a_sl, n, eval, evec, mixed->max_iters,
+                                      mixed->tol, CUEV_PRODUCTS_INT8, stream, &ri));
+        auto wall2 = std::chrono::high_resolution_clock::now();
+        if (mixed->info) {
+            cuev_mixed_info &mi = *mixed->info;
+            mi.refine_iterations = ri.iterations;
+            mi.offdiag_fro = ri.offdiag_fro;
+            mi.orth_fro = ri.orth_fro;
+            mi.anorm = ri.anorm;
+            mi.first_ms = std::chrono::duration<float, std::milli>(wall1 - wall0).count();
+            mi.refine_ms = std::chrono::duration<float, std::milli>(wall2 - wall1).count();
+        }
+    }
     if (timer) {
         float t[5];
         for (int i = 0; i < 5; ++i) CUEV_TRY(cudaEventElapsedTime(&t[i], ev.e[i], ev.e[i + 1]));
@@ -195,6 +239,16 @@ extern "C" int cuev_dsyevd(double *A, int n, double *eval, double *evec, void *s
     return solve_d(A, n, eval, evec, (cudaStream_t)stream, timer, nullptr);
 }
 
+extern "C" int cuev_dsyevd_mixed(double *A, int n, double *eval, double *evec, void *stream,
+                                 cuev_timer *timer, int max_refine_iters, double tol,
+                                 cuev_mixed_info *info) {
+    if (max_refine_iters < 0) return CUEV_ERR_INVALID;
+    if (info) *info = cuev_mixed_info{};
+    if (n == 1) return solve_d(A, n, eval, evec, (cudaStream_t)stream, timer, nullptr);
+    MixedReq req{max_refine_iters, tol, info};
+    return solve_d(A, n, eval, evec, (cudaStream_t)stream, timer, nullptr, &req);
+}
+
 extern "C" int cuev_ssyevd(float *A, int n, float *eval, float *evec, void *stream,
                            cuev_timer *timer) {
     if (n < 0) return CUEV_ERR_INVALID;
@@ -226,7 +280,6 @@ extern "C" int cuev_release_workspace(void) {
     std::lock_guard<std::mutex> lk(g_cache_mu);
     for (auto &c : g_cache) {
         if (c.ws && !c.busy) {
-            cudaDeviceSynchronize();
             workspace_destroy(c.ws);
             c.ws = nullptr;
         }
@@ -274,6 +327,7 @@ extern "C" int cuev_handle_buffer(cuev_handle h, int which, void **ptr, long lon
 #define HCHECK(h)                                                                                  \
     do {                                                                                           \
         if (!(h) || !(h)->ws) return CUEV_ERR_INVALID;                                             \
+        CUEV_CHECK_STATUS(apply_wait_limit((h)->ws->status, (h)->ws->stream));                     \
     } while (0)
 
 extern "C" int cuev_dbbr_panel_qr(cuev_handle h, double *A, int lda, double *Y, int ldy,
@@ -348,7 +402,7 @@ extern "C" int cuev_back_transform(cuev_handle h, double *evec, cuev_timer *time
         CUEV_TRY(cudaEventElapsedTime(&timer->bt_qs_ms, ev.e[1], ev.e[2]));
         timer->bt_ms = timer->bt_qb_ms + timer->bt_qs_ms;
     }
-    return CUEV_OK;
+    return workspace_check_status(ws, "back_transform");
 }
 
 // ---------------------------------------------------------------------------------------------

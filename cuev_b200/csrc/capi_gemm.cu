@@ -113,6 +113,7 @@ extern "C" int cuev_dgemm_i8(void *stream, int ta, int tb, int m, int n, int k, 
     CUEV_CHECK_STATUS(scratch_get(need, &scr, st));
     int *status = (int *)((char *)scr + need - 256);
     CUEV_TRY(cudaMemsetAsync(status, 0, sizeof(int) * DEV_STATUS_WORDS, st));
+    CUEV_CHECK_STATUS(apply_wait_limit(status, st));
     CUEV_CHECK_STATUS(i8_dgemm(ta, tb, 0, m, n, k, slices, alpha, A, lda, B, ldb, beta, C, ldc, 0,
                                scr, status, st));
     int host[DEV_STATUS_WORDS] = {0};

@@ -11,6 +11,11 @@
 // The array is NOALLOC_SCRATCH_DOUBLES doubles (16 MiB) of device memory; every GPU that loads
 // the library holds it until the process exits.  A call needs 2 * m * n doubles of it at least
 // (a two-way split of K), so m * n is limited to NOALLOC_MAX_MN = 1,048,576.
+//
+// When the 16 MiB are committed: with lazy module loading (CUDA_MODULE_LOADING=LAZY, the default
+// since CUDA 12) the array is created when the library's module is first loaded on a device,
+// which can be this entry's first call there.  A caller whose framework reserves most of the
+// device memory up front should make one call (a warm-up) before the framework takes its pool.
 #include "common.cuh"
 #include "gemm.cuh"
 
@@ -62,8 +67,14 @@ using namespace cuev;
 extern "C" int cuev_dgemm_noalloc(void *stream, int ta, int tb, int m, int n, int k, double alpha,
                                   const double *A, int lda, const double *B, int ldb, double beta,
                                   double *C, int ldc) {
-    if (m < 0 || n < 0 || k < 0 || !C || (k > 0 && (!A || !B))) return CUEV_ERR_INVALID;
-    if (ldc < m || lda < (ta ? k : m) || ldb < (tb ? n : k)) return CUEV_ERR_INVALID;
+    if (m < 0 || n < 0 || k < 0 || !C || (k > 0 && (!A || !B))) {
+        set_last_message("cuev_dgemm_noalloc: negative size or null pointer");
+        return CUEV_ERR_INVALID;
+    }
+    if (ldc < m || lda < (ta ? k : m) || ldb < (tb ? n : k)) {
+        set_last_message("cuev_dgemm_noalloc: leading dimension smaller than the matrix");
+        return CUEV_ERR_INVALID;
+    }
     if ((size_t)m * (size_t)n > NOALLOC_MAX_MN) {
         char msg[200];
         snprintf(msg, sizeof(msg),

@@ -44,10 +44,19 @@ size_t max_dynamic_smem(const void *func);
 
 // Device status word layout (one int per failure class; first writer wins).
 enum DevStatusSlot : int {
-    DEV_STATUS_CODE = 0,  // a cuev_status code, 0 = ok
-    DEV_STATUS_WHERE = 1, // kernel-specific detail (e.g. sweep index that timed out)
+    DEV_STATUS_CODE = 0,      // a cuev_status code, 0 = ok
+    DEV_STATUS_WHERE = 1,     // kernel-specific detail (e.g. sweep index that timed out)
+    DEV_STATUS_LIMIT_LO = 2,  // bounded-wait limit in ns (low, high word); 0 = the default 2 s.
+    DEV_STATUS_LIMIT_HI = 3,  // Only cuev_debug_set_wait_limit_ns sets it (failure-path tests).
     DEV_STATUS_WORDS = 4
 };
+
+// cudaFuncSetAttribute(MaxDynamicSharedMemorySize) applies to the current device only: set it
+// once per (kernel, device).
+int ensure_dyn_smem(const void *func, size_t bytes);
+// Write the wait limit chosen by cuev_debug_set_wait_limit_ns into status words 2-3 (stream
+// ordered; no-op while the limit is the default).
+int apply_wait_limit(int *status, cudaStream_t stream);
 
 #ifdef __CUDACC__
 
@@ -55,6 +64,13 @@ __device__ __forceinline__ uint64_t global_ns() {
     uint64_t t;
     asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
     return t;
+}
+
+/// Limit of a bounded wait: 2 s unless a failure-path test lowered it (status words 2-3).
+__device__ __forceinline__ uint64_t wait_limit_ns(const int *status) {
+    const uint64_t v = ((uint64_t)(unsigned)status[DEV_STATUS_LIMIT_HI] << 32) |
+                       (unsigned)status[DEV_STATUS_LIMIT_LO];
+    return v ? v : 2000000000ull;
 }
 
 /// Record a device-side failure (first failure wins); never traps.
@@ -126,7 +142,8 @@ struct GridBarrier {
     }
 
     /// Returns true on success.  Must be called by all threads of every CTA.
-    __device__ bool sync(int *status, int where, uint64_t limit_ns = 2000000000ull) {
+    __device__ bool sync(int *status, int where) {
+        const uint64_t limit_ns = wait_limit_ns(status);
         __shared__ int s_ok;
         __syncthreads();
         if (threadIdx.x == 0) {

@@ -481,12 +481,7 @@ template <int BW> int launch_panel_qr(Workspace *ws, double *A, long long lda, d
         return CUEV_ERR_INVALID;
     }
     const size_t smem = panel_qr_smem<BW>(chunk);
-    static bool attr = false;
-    if (!attr) {
-        CUEV_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)max_smem));
-        attr = true;
-    }
+    CUEV_CHECK_STATUS(ensure_dyn_smem((const void *)kern, max_smem));
     CUEV_TRY(cudaMemsetAsync(ws->bar, 0, 2 * sizeof(unsigned), ws->stream));
     void *args[] = {&A, &lda, &Y, &ldy, &tau, &T, &W, &ldw, &rows, &b, &chunk,
                     &ws->qr_part, &ws->bar, &ws->status};

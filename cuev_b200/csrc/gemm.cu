@@ -411,12 +411,7 @@ template <class C, bool TA, bool TB, bool SYMM, bool BATCHED, int VEC>
 int launch_cfg(const GemmArgs &a, const GemmArgs *dev_args, dim3 grid, cudaStream_t stream) {
     using L = SmemLayout<C, TA, TB, SYMM>;
     auto kern = dgemm_kernel<C, TA, TB, SYMM, BATCHED, VEC>;
-    static bool attr_set = false; // one attribute call per instantiation and process
-    if (!attr_set) {
-        CUEV_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)L::BYTES));
-        attr_set = true;
-    }
+    CUEV_CHECK_STATUS(ensure_dyn_smem((const void *)kern, L::BYTES));
     kern<<<grid, C::NT, L::BYTES, stream>>>(a, dev_args); note_launch();
     CUEV_TRY(cudaGetLastError());
     return CUEV_OK;
@@ -516,7 +511,8 @@ int gemm_launch(const GemmArgs &a_in, int ta, int tb, cudaStream_t stream) {
     const int ktot = a.k + a.k2;
     if (ktot <= 0 || a.alpha == 0.0) {
         // C = beta C on the (masked) output; reuse the reduction kernel with zero splits.
-        splitk_reduce_kernel<<<std::min(4096, div_up(a.m * a.n, 256)), 256, 0, stream>>>(
+        const long long mn = (long long)a.m * a.n;
+        splitk_reduce_kernel<<<(int)std::min<long long>(4096, (mn + 255) / 256), 256, 0, stream>>>(
             a.m, a.n, 0, nullptr, a.beta, a.C, a.ldc, a.c_lower); note_launch();
         CUEV_TRY(cudaGetLastError());
         return CUEV_OK;

@@ -71,8 +71,9 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
     return ok != 0;
 }
 
-// Bounded wait for the phase of parity `parity` of `bar`.  Gives up after 2 s (or when another
-// role has given up), recording CUEV_ERR_TIMEOUT.
+// Bounded wait for the phase of parity `parity` of `bar`.  Gives up after 2 s (the status words'
+// limit, lowered only by failure-path tests) or when another role has given up, recording
+// CUEV_ERR_TIMEOUT.
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int *abort_flag,
                                           int *status, int where) {
     uint64_t t0 = 0;
@@ -83,7 +84,7 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatil
             const uint64_t t = global_ns();
             if (t0 == 0) {
                 t0 = t;
-            } else if (t - t0 > 2000000000ull) {
+            } else if (t - t0 > wait_limit_ns(status)) {
                 *abort_flag = 1;
                 dev_fail(status, CUEV_ERR_TIMEOUT, where);
                 return false;
@@ -396,17 +397,30 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                         }
                         const int cb = col0 + 32 * c;
                         const int fe = (cb + lane < a.n) ? a.eb[cb + lane] : 0;
+                        // all 32 reads of C first (independent, in flight together), then the
+                        // updates: interleaving them would serialise every read behind the
+                        // previous store (they may alias as far as the compiler knows)
+                        const bool need_old = !first || a.beta != 0.0;
 #pragma unroll
-                        for (int r = 0; r < 32; ++r) {
-                            const int col = cb + r;
-                            const int fc = __shfl_sync(0xffffffffu, fe, r);
-                            if (!row_ok || col >= a.n || (a.c_lower && row < col)) continue;
-                            const double val = (double)(int)v[r] * rs * pow2i(fc);
-                            double *cp = crow + (long long)col * a.ldc;
-                            if (first)
-                                *cp = (a.beta != 0.0) ? val + a.beta * (*cp) : val;
-                            else
-                                *cp += val;
+                        for (int h = 0; h < 32; h += 16) {
+                            double old[16];
+#pragma unroll
+                            for (int r = 0; r < 16; ++r) {
+                                const int col = cb + h + r;
+                                const bool ok_el =
+                                    row_ok && col < a.n && !(a.c_lower && row < col);
+                                old[r] = (need_old && ok_el) ? crow[(long long)col * a.ldc] : 0.0;
+                            }
+#pragma unroll
+                            for (int r = 0; r < 16; ++r) {
+                                const int col = cb + h + r;
+                                const int fc = __shfl_sync(0xffffffffu, fe, h + r);
+                                if (!row_ok || col >= a.n || (a.c_lower && row < col)) continue;
+                                const double val = (double)(int)v[h + r] * rs * pow2i(fc);
+                                crow[(long long)col * a.ldc] =
+                                    first ? (a.beta != 0.0 ? val + a.beta * old[r] : val)
+                                          : old[r] + val;
+                            }
                         }
                     }
                     first = false;
@@ -561,23 +575,10 @@ int make_map(const I8Operand &op, int box_rows, CUtensorMap *map) {
     return CUEV_OK;
 }
 
-std::mutex g_attr_mu;
-unsigned long long g_attr_done[2] = {0ull, 0ull}; // bit dev per BN variant
-
 template <int BN> int launch_i8(const CUtensorMap &ma, const CUtensorMap &mb, const TcArgs &a,
                                 int grid, cudaStream_t st) {
     auto kern = i8_gemm_kernel<BN>;
-    int dev = 0;
-    CUEV_TRY(cudaGetDevice(&dev));
-    {
-        std::lock_guard<std::mutex> lk(g_attr_mu);
-        unsigned long long &done = g_attr_done[BN == 256 ? 1 : 0];
-        if (dev < 0 || dev >= 64 || !(done >> dev & 1ull)) {
-            CUEV_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          TcCfg<BN>::SMEM));
-            if (dev >= 0 && dev < 64) done |= 1ull << dev;
-        }
-    }
+    CUEV_CHECK_STATUS(ensure_dyn_smem((const void *)kern, TcCfg<BN>::SMEM));
     kern<<<grid, TC_THREADS, TcCfg<BN>::SMEM, st>>>(ma, mb, a);
     note_launch();
     CUEV_TRY(cudaGetLastError());

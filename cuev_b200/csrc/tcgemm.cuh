@@ -20,6 +20,11 @@
 
 namespace cuev {
 
+// Slices of the precision form's stage GEMMs (FP32-level: 2^-28 relative to the row and column
+// maxima) and of its refinement measurements (FP64-level).
+constexpr int MIXED_SLICES = 4;
+constexpr int RF_SLICES_HI = 7;
+
 // int8 slices of one GEMM operand op(X) (rows x k), K-major: byte (r, kk) of slice p (0-based) is
 // data[p * slice_stride + r * k_ld + kk]; k_ld is k rounded up to 128 and the padding is zero.
 struct I8Operand {

@@ -100,8 +100,37 @@ int workspace_create(int n, int b, int k, cudaStream_t stream, Workspace **out) 
     return CUEV_OK;
 }
 
+// Slices of A for the refinement (FP64-level), the operands of the largest mixed GEMM (the
+// SBR-back's Y^T M: k x n by n x n at FP32-level slices) and an FP32 n x n matrix.
+int workspace_enable_mixed(Workspace *ws) {
+    if (ws->mx_pool) return CUEV_OK;
+    const int n = std::max(ws->n, 1);
+    const size_t a_bytes = i8_operand_bytes(n, n, RF_SLICES_HI);
+    const size_t g_bytes = i8_gemm_scratch_bytes(std::max(ws->k, n), n, n, MIXED_SLICES);
+    const size_t f_bytes = sizeof(float) * (size_t)n * n;
+    const size_t total = align256(a_bytes) + align256(g_bytes) + align256(f_bytes);
+    if (cudaMalloc(&ws->mx_pool, total) != cudaSuccess) {
+        cudaGetLastError();
+        ws->mx_pool = nullptr;
+        char msg[160];
+        snprintf(msg, sizeof(msg), "precision form: allocation of %.2f GB failed", total / 1e9);
+        set_last_message(msg);
+        return CUEV_ERR_ALLOC;
+    }
+    ws->mx_bytes = total;
+    char *p = (char *)ws->mx_pool;
+    i8_operand_init(p, n, n, RF_SLICES_HI, ws->a_sl);
+    p += align256(a_bytes);
+    ws->i8_scratch = p;
+    ws->i8_scratch_bytes = g_bytes;
+    p += align256(g_bytes);
+    ws->m32 = (float *)p;
+    return CUEV_OK;
+}
+
 void workspace_destroy(Workspace *ws) {
     if (!ws) return;
+    if (ws->mx_pool) cudaFree(ws->mx_pool);
     if (ws->side) cudaStreamSynchronize(ws->side), cudaStreamDestroy(ws->side);
     if (ws->ev_a) cudaEventDestroy(ws->ev_a);
     if (ws->ev_b) cudaEventDestroy(ws->ev_b);

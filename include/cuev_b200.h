@@ -114,6 +114,41 @@ typedef struct cuev_refine_info {
 int cuev_dsyev_refine(const double *A, int n, double *eval, double *evec, int max_iters,
                       double tol, void *stream, cuev_refine_info *info);
 
+/* Arithmetic of the refinement's n x n products. */
+typedef enum cuev_products {
+    CUEV_PRODUCTS_FP64 = 0, /* FP64 DMMA (7 n^3 flop per step) */
+    CUEV_PRODUCTS_INT8 = 1  /* int8 tensor cores (tcgen05.mma.kind::i8) with 7-bit operand slices:
+                               A X, X^T A X and X^T X from 7 slices per operand (FP64-level, error
+                               ~ 2^-49 relative to the row and column maxima), the correction X E
+                               from 5; X^T X and X^T A X are formed as lower triangles */
+} cuev_products;
+/* cuev_dsyev_refine with a choice of product arithmetic (no reference counterpart). */
+int cuev_dsyev_refine_ex(const double *A, int n, double *eval, double *evec, int max_iters,
+                         double tol, int products, void *stream, cuev_refine_info *info);
+
+/* Precision form (no reference counterpart; the north star's mixed+refine solve).  Same
+ * arguments and result as cuev_dsyevd (A overwritten, eval ascending, evec columns), computed
+ * in two parts:
+ *   1. a first solve whose back-transform products Y^T M, T X and Y X (SBR-back, each of at
+ *      least 2^30 multiply-adds) run on the int8 tensor cores at FP32-level accuracy (4 slices);
+ *      the band reduction, bulge chase, D&C and BC-back stay FP64;
+ *   2. Ogita-Aishima refinement of those eigenpairs against the original A with FP64-level
+ *      int8 tensor-core products (CUEV_PRODUCTS_INT8), at most max_refine_iters steps, stopping
+ *      once ||I - X^T X||_F <= tol and ||X^T A X - diag||_F <= tol max|lam| (tol <= 0: all steps).
+ * The original A is kept as int8 slices before the first part overwrites it.  info and timer may
+ * be NULL; timer holds the first part's stages.  Blocks until done. */
+typedef struct cuev_mixed_info {
+    int refine_iterations; /* refinement steps applied */
+    double offdiag_fro;    /* ||X^T A X - diag(lam)||_F at the last measurement */
+    double orth_fro;       /* ||I - X^T X||_F at the last measurement */
+    double anorm;          /* max |lam_i| */
+    float first_ms;        /* first solve, incl. slicing A */
+    float refine_ms;       /* refinement */
+} cuev_mixed_info;
+int cuev_dsyevd_mixed(double *A, int n, double *eval, double *evec, void *stream,
+                      cuev_timer *timer, int max_refine_iters, double tol,
+                      cuev_mixed_info *info);
+
 /* Release the cached device workspace (the solves keep one pool per (n, b, k) between calls). */
 int cuev_release_workspace(void);
 
@@ -122,6 +157,14 @@ const char *cuev_last_error(void);
 
 /* Number of CUDA kernels this library has launched since it was loaded (profiling aid). */
 long long cuev_kernel_launches(void);
+
+/* Failure-path testing (no reference counterpart; the reference has no bounded waits).  Every
+ * device-side wait of the library (bulge-chase hand-off, grid barriers, BC-back's warp pipeline,
+ * the tensor-core GEMM's mbarriers) gives up after 2 s and the call returns CUEV_ERR_TIMEOUT.
+ * This sets that limit for the calls that follow (0 restores 2 s), so a test can make the waits
+ * run out on purpose and check that the error is reported and the next call succeeds.  Not
+ * meant for production use: a short limit turns ordinary waiting into failures. */
+int cuev_debug_set_wait_limit_ns(unsigned long long ns);
 
 /* ---------------------------------------------------------------------------------------------
  * Stage-level API used by the stage tests.  Mirrors the reference's SolverHandle<T> and
@@ -182,7 +225,8 @@ int cuev_bc_back(cuev_handle h, double *M, int ldm);
 /* M <- Q_s M (n x n, ld ldm).  Replaces kernels::sbr_back (reference src/cuda/backtransform.cu:210-230). */
 int cuev_sbr_back(cuev_handle h, double *M, int ldm);
 
-/* evec <- Q_s Q_b evec.  Replaces kernels::back_transform (reference src/cuda/backtransform.cu:232-275). */
+/* evec <- Q_s Q_b evec.  Replaces kernels::back_transform (reference src/cuda/backtransform.cu:232-275).
+ * Blocks until done and returns CUEV_ERR_TIMEOUT if one of BC-back's bounded waits gave up. */
 int cuev_back_transform(cuev_handle h, double *evec, cuev_timer *timer);
 
 /* FP64 tensor-core GEMM used by every stage: C = alpha op(A) op(B) + beta C (column-major).
@@ -208,6 +252,16 @@ int cuev_dgemm(void *stream, int ta, int tb, int m, int n, int k, double alpha, 
 int cuev_dgemm_noalloc(void *stream, int ta, int tb, int m, int n, int k, double alpha,
                        const double *A, int lda, const double *B, int ldb, double beta, double *C,
                        int ldc);
+
+/* Same product as cuev_dgemm emulated on the int8 tensor cores (no reference counterpart):
+ * every row of op(A) and column of op(B) is scaled by a power of two and cut into `slices`
+ * (1..8) signed 7-bit integer slices; the slice products run as tcgen05.mma.kind::i8 with int32
+ * accumulation in TMEM and are summed in FP64.  Error per entry ~ 14 2^(-7 slices) sqrt(k)
+ * rowmax_i(op(A)) colmax_j(op(B)): 7 slices give FP64-level, 4 FP32-level products.  Slices
+ * live in the same per-device scratch as cuev_dgemm's split-K partials.  Blocks until done. */
+int cuev_dgemm_i8(void *stream, int ta, int tb, int m, int n, int k, int slices, double alpha,
+                  const double *A, int lda, const double *B, int ldb, double beta, double *C,
+                  int ldc);
 
 /* C = alpha A B + beta C with A symmetric (m x m, lower triangle read).  Replaces
  * cuev::cublas::symm(LEFT, LOWER) (reference src/cuda/cublas.cu:28-37). */

@@ -2,8 +2,10 @@
 oracle/ref/Makefile into oracle/_ref/) on seeded inputs.  Runs on a GPU machine; writes
   tests/golden/ref_eig_n{n}.npz   eval (and evec for n=256) of A = (G + G^T)/2, G from
                                   numpy default_rng(n).standard_normal((n, n))
+  tests/golden/ref_eval_n{n}.npz  eval only, same input, at the large sizes (--eval-sizes)
   <out>/ref_timings.jsonl         the reference's SolveTimer per size
-Usage: python tests/golden/make_ref_golden.py [--out DIR] [--timing-sizes 1024,4096,...]
+Usage: python tests/golden/make_ref_golden.py [--out DIR] [--golden-sizes ...]
+                                              [--eval-sizes 8192,16384] [--timing-sizes ...]
 """
 import argparse
 import json
@@ -29,7 +31,7 @@ def run_ref(A: np.ndarray, want_vec: bool, timeout: int):
     with tempfile.TemporaryDirectory() as td:
         fin, fw, fv = (os.path.join(td, x) for x in ("A.bin", "w.bin", "V.bin"))
         np.asfortranarray(A).ravel(order="F").tofile(fin)
-        cmd = [str(DRIVER), str(n), fin, fw] + ([fv] if want_vec else [])
+        cmd = [str(DRIVER), str(n), fin, fw, fv if want_vec else "-"]
         res = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout)
         if res.returncode != 0:
             raise RuntimeError(f"reference failed (n={n}): {res.stderr[-500:]}")
@@ -41,9 +43,10 @@ def run_ref(A: np.ndarray, want_vec: bool, timeout: int):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--out", default=str(ROOT / "gpurun_out"))
+    ap.add_argument("--out", default=str(ROOT / "tests" / "golden"))
     ap.add_argument("--golden-sizes", default="256,512,1024")
-    ap.add_argument("--timing-sizes", default="1024,4096,8192,16384")
+    ap.add_argument("--eval-sizes", default="8192,16384")
+    ap.add_argument("--timing-sizes", default="")
     ap.add_argument("--timeout", type=int, default=600)
     args = ap.parse_args()
     out = Path(args.out)
@@ -60,6 +63,11 @@ def main():
             payload["evec_sample"] = V[:, cols]
         np.savez_compressed(out / f"ref_eig_n{n}.npz", **payload)
         print(json.dumps({"golden": n, **timer}), flush=True)
+    for n in [int(x) for x in args.eval_sizes.split(",") if x]:
+        A = sym_input(n)
+        w, _, timer = run_ref(A, False, args.timeout)
+        np.savez_compressed(out / f"ref_eval_n{n}.npz", n=n, eval=w, seed=n)
+        print(json.dumps({"golden_eval": n, **timer}), flush=True)
     with open(out / "ref_timings.jsonl", "a") as fh:
         for n in [int(x) for x in args.timing_sizes.split(",") if x]:
             A = sym_input(n)

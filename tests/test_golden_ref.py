@@ -60,3 +60,24 @@ def test_library_matches_reference_outputs(cuda, n):
     wh = w.cpu().numpy()
     assert np.abs(wh - wr).max() / np.abs(wr).max() < 1e-13
     _check_vectors(g, V.cpu().numpy().reshape((n, n)).T)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [8192, 16384])
+def test_library_matches_reference_eigenvalues_large(cuda, n):
+    """Parity at the bench sizes: the reference's own eigenvalues of the same seeded matrix
+    (tests/golden/ref_eval_n{n}.npz, b = 32 as the reference hard-codes) within 1e-12 relative."""
+    import torch
+    import cuev_b200 as cv
+    f = GOLD / f"ref_eval_n{n}.npz"
+    assert f.exists(), f"missing golden fixture {f.name}"
+    wr = np.load(f)["eval"]
+    A = _input(n)
+    dA = torch.from_numpy(A.ravel(order="F").copy()).to(cuda)
+    del A
+    w = torch.zeros(n, dtype=torch.float64, device=cuda)
+    V = torch.zeros(n * n, dtype=torch.float64, device=cuda)
+    cv.symm_eig_solve(dA, n, w, V)
+    torch.cuda.synchronize()
+    wh = w.cpu().numpy()
+    assert np.abs(wh - wr).max() / np.abs(wr).max() < 1e-12
