@@ -20,9 +20,12 @@
 
 namespace cuev {
 
-// Slices of the precision form's stage GEMMs (FP32-level: 2^-28 relative to the row and column
-// maxima) and of its refinement measurements (FP64-level).
-constexpr int MIXED_SLICES = 4;
+// Slices of the precision form's stage GEMMs and of its refinement measurements.  The stage
+// products are those of the back-transform, whose Householder operand rows hold a unit entry
+// next to entries of order 1/sqrt(n): the row scaling is set by the unit entry, so 5 slices
+// (35 bits of the row maximum) leave about FP32-level accuracy (2^-28) for the small entries,
+// which is what one refinement step needs to reach a residual of 1e-13.
+constexpr int MIXED_SLICES = 5;
 constexpr int RF_SLICES_HI = 7;
 
 // int8 slices of one GEMM operand op(X) (rows x k), K-major: byte (r, kk) of slice p (0-based) is

@@ -130,7 +130,8 @@ int cuev_dsyev_refine_ex(const double *A, int n, double *eval, double *evec, int
  * arguments and result as cuev_dsyevd (A overwritten, eval ascending, evec columns), computed
  * in two parts:
  *   1. a first solve whose back-transform products Y^T M, T X and Y X (SBR-back, each of at
- *      least 2^30 multiply-adds) run on the int8 tensor cores at FP32-level accuracy (4 slices);
+ *      least 2^30 multiply-adds) run on the int8 tensor cores at FP32-level accuracy (5 slices;
+ *      the reflectors' unit entries set their rows' scale, so 5 slices leave ~2^-28 for the rest);
  *      the band reduction, bulge chase, D&C and BC-back stay FP64;
  *   2. Ogita-Aishima refinement of those eigenpairs against the original A with FP64-level
  *      int8 tensor-core products (CUEV_PRODUCTS_INT8), at most max_refine_iters steps, stopping
