@@ -55,8 +55,12 @@ def _sym(n, seed, dev):
     return ((G + G.t()) / 2).to(dev)
 
 
-@pytest.mark.parametrize("n", [64, 300, 1024])
+@pytest.mark.parametrize("n", [64, 300, 1024, 4096])
 def test_adjoint_vs_torch_eigh(cuda, n):
+    """Against torch.linalg.eigh's gradient, up to n = 4096 (the differentiation config).  Both
+    gradients carry each solver's eigenvector rounding divided by the smallest eigenvalue gaps
+    (F_ij = 1/(lam_j - lam_i)); for A = (G + G^T)/2 the smallest gap relative to ||A|| shrinks as
+    n^(-3/2), so the bound grows from 1e-10 at n <= 1024 to 1e-9 at n = 4096."""
     import torch
     eigh = _make_eigh()
     A = _sym(n, n, cuda).requires_grad_(True)
@@ -72,7 +76,7 @@ def test_adjoint_vs_torch_eigh(cuda, n):
     gt = A2.grad
     # torch returns the gradient w.r.t. the symmetric input; both are symmetric here
     rel = (ga - gt).norm() / gt.norm()
-    assert rel < 1e-10, rel.item()
+    assert rel < (1e-10 if n <= 1024 else 1e-9), rel.item()
     assert (ga - ga.t()).abs().max() < 1e-12 * ga.abs().max()
 
 

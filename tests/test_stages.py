@@ -136,6 +136,11 @@ def test_backtransform_vs_oracle(cuda, n, b, k):
         Qs = _np_cm(Ms, n, n)
     Qb_o = O.bc_back(Ug, np.eye(n), b)
     assert np.abs(Qb - Qb_o).max() < 1e-12
+    # SBR-back beside the oracle's (reference backtransform.cu:210-230 restated): the oracle's
+    # band reduction of the same input, its reflectors applied panel by panel to I
+    _, Yo, Wo, _ = O.dbbr_reduce(A0, b, k)
+    Qs_o = O.sbr_back(Yo, Wo, np.eye(n), b)
+    assert np.abs(Qs - Qs_o).max() < 1e-10, np.abs(Qs - Qs_o).max()
     rb = np.linalg.norm(Qb.T @ Band @ Qb - Tri) / np.linalg.norm(Tri)
     assert rb < 1e-9
     rs = np.linalg.norm(Qs.T @ A @ Qs - Band) / np.linalg.norm(Band)
