@@ -111,9 +111,11 @@ struct MixedFlag {
     }
 };
 
-// mixed == nullptr: the plain FP64 solve.  Otherwise the precision form: A's FP64-level slices
-// are taken first, the solve runs with ws->mixed set, then the eigenpairs are refined.
+// mixed == nullptr: the plain FP64 solve.  Otherwise the solve runs with ws->mixed set (the
+// back-transform on FP32-level tensor-core products) and, when `refine` is set (the precision
+// form), A's FP64-level slices are taken first and the eigenpairs are refined afterwards.
 struct MixedReq {
+    bool refine;
     int max_iters;
     double tol;
     cuev_mixed_info *info;
@@ -157,9 +159,9 @@ int solve_d(double *A, int n, double *eval, double *evec, cudaStream_t stream, c
 
     MixedFlag mflag{nullptr};
     if (mixed) {
-        CUEV_CHECK_STATUS(workspace_enable_mixed(ws));
+        CUEV_CHECK_STATUS(workspace_enable_mixed(ws, mixed->refine));
         // the refinement measures against the original A: keep it as FP64-level slices
-        CUEV_CHECK_STATUS(i8_slice(A, n, I8_SRC_SYML, ws->a_sl, stream));
+        if (mixed->refine) CUEV_CHECK_STATUS(i8_slice(A, n, I8_SRC_SYML, ws->a_sl, stream));
         ws->mixed = 1;
         mflag.ws = ws;
     }
@@ -181,7 +183,7 @@ int solve_d(double *A, int n, double *eval, double *evec, cudaStream_t stream, c
     CUEV_CHECK_STATUS(rec(5));
     CUEV_CHECK_STATUS(workspace_check_status(ws, "solve"));
     auto wall1 = std::chrono::high_resolution_clock::now();
-    if (mixed) {
+    if (mixed && mixed->refine) {
         ws->mixed = 0;
         cuev_refine_info ri{};
         CUEV_CHECK_STATUS(refine_core(nullptr, &ws->a_sl, n, eval, evec, mixed->max_iters,
@@ -245,7 +247,7 @@ extern "C" int cuev_dsyevd_mixed(double *A, int n, double *eval, double *evec, v
     if (max_refine_iters < 0) return CUEV_ERR_INVALID;
     if (info) *info = cuev_mixed_info{};
     if (n == 1) return solve_d(A, n, eval, evec, (cudaStream_t)stream, timer, nullptr);
-    MixedReq req{max_refine_iters, tol, info};
+    MixedReq req{true, max_refine_iters, tol, info};
     return solve_d(A, n, eval, evec, (cudaStream_t)stream, timer, nullptr, &req);
 }
 
@@ -265,7 +267,11 @@ extern "C" int cuev_ssyevd(float *A, int n, float *eval, float *evec, void *stre
     double *A64 = buf, *V64 = buf + nn, *w64 = buf + 2 * nn;
     const int blocks = 4 * num_sms();
     widen_kernel<<<blocks, 256, 0, st>>>(A, A64, nn); note_launch();
-    int s = solve_d(A64, n, w64, evec ? V64 : nullptr, st, timer, nullptr);
+    // FP32 results need FP32 accuracy only: the back-transform's large products run on the int8
+    // tensor cores at FP32 level (the precision form's first solve, without refinement)
+    MixedReq first_only{false, 0, 0.0, nullptr};
+    int s = solve_d(A64, n, w64, evec ? V64 : nullptr, st, timer, nullptr,
+                    evec ? &first_only : nullptr);
     if (s == CUEV_OK) {
         if (evec) { narrow_kernel<<<blocks, 256, 0, st>>>(V64, evec, nn); note_launch(); }
         narrow_kernel<<<1, 256, 0, st>>>(w64, eval, n); note_launch();

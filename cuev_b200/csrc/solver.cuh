@@ -49,17 +49,17 @@ struct Workspace {
 
     double *tmp_nn = nullptr; // n x n scratch (back-transform / D&C output staging)
 
-    // Precision form (cuev_dsyevd_mixed): while `mixed` is set, the large GEMMs of the stages run
-    // as FP32-level int8 tensor-core products (MIXED_SLICES slices) and BC-back in FP32.  Its
-    // buffers are allocated on the first mixed solve: A's FP64-level slices for the refinement
-    // (taken before the band reduction overwrites A) and the slices of one GEMM's operands.
+    // Precision form (cuev_dsyevd_mixed) and the FP32 entry: while `mixed` is set, the
+    // back-transform's large GEMMs run as FP32-level int8 tensor-core products (MIXED_SLICES
+    // slices).  Buffers are allocated on first use: the slices of one GEMM's operands and, for the
+    // refinement, A's FP64-level slices (taken before the band reduction overwrites A).
     int mixed = 0;
     void *mx_pool = nullptr;
     size_t mx_bytes = 0;
+    bool mx_has_a = false;
     I8Operand a_sl;
     void *i8_scratch = nullptr;
     size_t i8_scratch_bytes = 0;
-    float *m32 = nullptr; // n x n FP32 copy of the back-transform's M (FP32 BC-back)
 
     void *pool = nullptr;
     size_t pool_bytes = 0;
@@ -67,8 +67,8 @@ struct Workspace {
 
 // Allocation / release of a workspace for (n, b, k).
 int workspace_create(int n, int b, int k, cudaStream_t stream, Workspace **out);
-// Allocate the precision form's buffers (once per workspace).
-int workspace_enable_mixed(Workspace *ws);
+// Allocate the precision form's buffers (GEMM slices; with_a_slices: also A's slices).
+int workspace_enable_mixed(Workspace *ws, bool with_a_slices);
 void workspace_destroy(Workspace *ws);
 // Check the device status word (synchronises the stream); returns its cuev_status.
 int workspace_check_status(Workspace *ws, const char *stage);

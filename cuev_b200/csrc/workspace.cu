@@ -100,15 +100,19 @@ int workspace_create(int n, int b, int k, cudaStream_t stream, Workspace **out) 
     return CUEV_OK;
 }
 
-// Slices of A for the refinement (FP64-level), the operands of the largest mixed GEMM (the
-// SBR-back's Y^T M: k x n by n x n at FP32-level slices) and an FP32 n x n matrix.
-int workspace_enable_mixed(Workspace *ws) {
-    if (ws->mx_pool) return CUEV_OK;
+// The operands of the largest mixed GEMM (the SBR-back's Y^T M: k x n by n x n, FP32-level
+// slices) and, for the refinement, A's FP64-level slices.
+int workspace_enable_mixed(Workspace *ws, bool with_a_slices) {
+    if (ws->mx_pool && (ws->mx_has_a || !with_a_slices)) return CUEV_OK;
+    if (ws->mx_pool) { // grow: A's slices were not allocated yet
+        CUEV_TRY(cudaStreamSynchronize(ws->stream));
+        cudaFree(ws->mx_pool);
+        ws->mx_pool = nullptr;
+    }
     const int n = std::max(ws->n, 1);
-    const size_t a_bytes = i8_operand_bytes(n, n, RF_SLICES_HI);
+    const size_t a_bytes = with_a_slices ? i8_operand_bytes(n, n, RF_SLICES_HI) : 0;
     const size_t g_bytes = i8_gemm_scratch_bytes(std::max(ws->k, n), n, n, MIXED_SLICES);
-    const size_t f_bytes = sizeof(float) * (size_t)n * n;
-    const size_t total = align256(a_bytes) + align256(g_bytes) + align256(f_bytes);
+    const size_t total = align256(a_bytes) + align256(g_bytes);
     if (cudaMalloc(&ws->mx_pool, total) != cudaSuccess) {
         cudaGetLastError();
         ws->mx_pool = nullptr;
@@ -118,13 +122,12 @@ int workspace_enable_mixed(Workspace *ws) {
         return CUEV_ERR_ALLOC;
     }
     ws->mx_bytes = total;
+    ws->mx_has_a = with_a_slices;
     char *p = (char *)ws->mx_pool;
-    i8_operand_init(p, n, n, RF_SLICES_HI, ws->a_sl);
-    p += align256(a_bytes);
     ws->i8_scratch = p;
     ws->i8_scratch_bytes = g_bytes;
     p += align256(g_bytes);
-    ws->m32 = (float *)p;
+    if (with_a_slices) i8_operand_init(p, n, n, RF_SLICES_HI, ws->a_sl);
     return CUEV_OK;
 }
 

@@ -73,7 +73,10 @@ int cuev_dsyevd_cfg(double *A, int n, double *eval, double *evec, void *stream, 
                     const cuev_config *cfg);
 
 /* FP32 interface.  Replaces cuev::symm_eig_solve<float> (reference src/cuda/solver.cu:78).
- * The float input is widened and solved by the FP64 pipeline, then rounded back. */
+ * The float input is widened and solved by the FP64 band reduction, bulge chase, D&C and
+ * BC-back, with the SBR-back products (the back-transform's GEMMs) on the int8 tensor cores at
+ * FP32-level accuracy (the precision form's first solve, cuev_dsyevd_mixed without refinement);
+ * the results are rounded back to FP32. */
 int cuev_ssyevd(float *A, int n, float *eval, float *evec, void *stream, cuev_timer *timer);
 
 /* Batched eigensolver for many small matrices (no reference counterpart: the reference solves one
