@@ -130,12 +130,16 @@ def lib() -> C.CDLL:
             fn.restype = C.c_int
         L.cuev_last_error.restype = C.c_char_p
         L.cuev_last_error.argtypes = []
+        if hasattr(L, "cuev_last_dc_flops"):
+            L.cuev_last_dc_flops.restype = C.c_double
+            L.cuev_last_dc_flops.argtypes = []
         _lib = L
     return _lib
 
 
 def exported_symbols() -> list[str]:
-    return [n for n in list(_SIGS) + ["cuev_last_error"] if hasattr(lib(), n)]
+    return [n for n in list(_SIGS) + ["cuev_last_error", "cuev_last_dc_flops"]
+            if hasattr(lib(), n)]
 
 
 def _check(status: int, where: str):

@@ -15,8 +15,11 @@
 // written in ascending order.
 //
 // Layout: A is batch x (n x n column-major, stride n^2), lower triangle read, not modified;
-// eval batch x n, evec batch x (n x n column-major).  A and V live in shared memory
-// (2 m (m + 1) doubles, m = n rounded up to even, 66 KB at n = 64).
+// eval batch x n, evec batch x (n x n column-major).  A and V live in shared memory, padded to
+// M x M with M in {8, 16, 32, 64} the smallest that holds n (2 M (M + 1) doubles, 66 KB at
+// M = 64); the padding rows and columns are zero and every pair with an index >= n is skipped, so
+// they never mix with the matrix.  M and the thread count (32, 64, 256, 256) are compile-time,
+// so the index arithmetic of the update loops is shifts and masks.
 #include "common.cuh"
 
 #include <mutex>
@@ -24,27 +27,27 @@
 namespace cuev {
 namespace {
 
-constexpr int BJ_THREADS = 256;
 constexpr int BJ_MAXN = 64;
 constexpr int BJ_MAX_SWEEPS = 60;
 
-__global__ void __launch_bounds__(BJ_THREADS)
+template <int M, int NT>
+__global__ void __launch_bounds__(NT)
     batched_jacobi_kernel(const double *__restrict__ A, int n, double *__restrict__ eval,
                           double *__restrict__ evec, int *__restrict__ status) {
     extern __shared__ __align__(16) double bj_smem[];
-    const int m = n + (n & 1); // even; index n is a dummy when n is odd
-    const int LD = m + 1;
-    double *sA = bj_smem;           // sA[i * LD + j] = A(i, j)
-    double *sV = sA + m * LD;       // sV[i * LD + j] = V(i, j)
-    __shared__ double cs_c[BJ_MAXN / 2], cs_s[BJ_MAXN / 2];
-    __shared__ int cs_p[BJ_MAXN / 2], cs_q[BJ_MAXN / 2];
+    constexpr int LD = M + 1;
+    constexpr int HALF = M / 2;
+    double *sA = bj_smem;     // sA[i * LD + j] = A(i, j)
+    double *sV = sA + M * LD; // sV[i * LD + j] = V(i, j)
+    __shared__ double cs_c[HALF], cs_s[HALF];
+    __shared__ int cs_p[HALF], cs_q[HALF];
     __shared__ int s_rot;
     const int tid = threadIdx.x;
     const long long bofs = (long long)blockIdx.x * n * n;
     const double *Ab = A + bofs;
 
-    for (int idx = tid; idx < m * m; idx += BJ_THREADS) {
-        const int i = idx % m, j = idx / m;
+    for (int idx = tid; idx < M * M; idx += NT) {
+        const int i = idx % M, j = idx / M;
         double v = 0.0;
         if (i < n && j < n) v = i >= j ? Ab[i + (long long)j * n] : Ab[j + (long long)i * n];
         sA[i * LD + j] = v;
@@ -54,18 +57,17 @@ __global__ void __launch_bounds__(BJ_THREADS)
 
     const double eps = 2.220446049250313e-16;
     const double tiny = 2.2250738585072014e-308;
-    const int half = m / 2;
-    bool converged = (m <= 1);
+    bool converged = (n <= 1);
     for (int sweep = 0; sweep < BJ_MAX_SWEEPS && !converged; ++sweep) {
         if (tid == 0) s_rot = 0;
         __syncthreads();
-        for (int r = 0; r < m - 1; ++r) {
-            // pairs of this round: slot 0 fixed, slots 1..m-1 rotate by r
-            if (tid < half) {
-                auto pos = [&](int slot) { return slot == 0 ? 0 : 1 + (slot - 1 + r) % (m - 1); };
-                int p = pos(tid), q = pos(m - 1 - tid);
+        for (int r = 0; r < M - 1; ++r) {
+            // pairs of this round: slot 0 fixed, slots 1..M-1 rotate by r
+            if (tid < HALF) {
+                auto pos = [&](int slot) { return slot == 0 ? 0 : 1 + (slot - 1 + r) % (M - 1); };
+                int p = pos(tid), q = pos(M - 1 - tid);
                 if (p > q) { const int x = p; p = q; q = x; }
-                double c = 1.0, s = 0.0;
+                double c = 1.0, sn = 0.0;
                 if (q < n) {
                     const double apq = sA[p * LD + q];
                     const double app = sA[p * LD + p], aqq = sA[q * LD + q];
@@ -74,42 +76,42 @@ __global__ void __launch_bounds__(BJ_THREADS)
                         const double t =
                             (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
                         c = 1.0 / sqrt(1.0 + t * t);
-                        s = t * c;
+                        sn = t * c;
                         atomicAdd(&s_rot, 1);
                     }
                 }
                 cs_p[tid] = p, cs_q[tid] = q;
-                cs_c[tid] = c, cs_s[tid] = s;
+                cs_c[tid] = c, cs_s[tid] = sn;
             }
             __syncthreads();
             // rows: A <- J^T A  (rows p, q of every column j)
-            for (int idx = tid; idx < half * m; idx += BJ_THREADS) {
-                const int k = idx / m, j = idx % m;
-                const double s = cs_s[k];
-                if (s == 0.0) continue;
+            for (int idx = tid; idx < HALF * M; idx += NT) {
+                const int k = idx / M, j = idx % M;
+                const double sn = cs_s[k];
+                if (sn == 0.0) continue;
                 const double c = cs_c[k];
                 const int p = cs_p[k], q = cs_q[k];
                 const double ap = sA[p * LD + j], aq = sA[q * LD + j];
-                sA[p * LD + j] = c * ap - s * aq;
-                sA[q * LD + j] = s * ap + c * aq;
+                sA[p * LD + j] = c * ap - sn * aq;
+                sA[q * LD + j] = sn * ap + c * aq;
             }
             __syncthreads();
             // columns: A <- A J, V <- V J  (columns p, q of every row i)
-            for (int idx = tid; idx < 2 * half * m; idx += BJ_THREADS) {
-                const int which = idx / (half * m), rem = idx % (half * m);
-                const int k = rem / m, i = rem % m;
-                const double s = cs_s[k];
-                if (s == 0.0) continue;
+            for (int idx = tid; idx < 2 * HALF * M; idx += NT) {
+                const int which = idx / (HALF * M), rem = idx % (HALF * M);
+                const int k = rem / M, i = rem % M;
+                const double sn = cs_s[k];
+                if (sn == 0.0) continue;
                 const double c = cs_c[k];
                 const int p = cs_p[k], q = cs_q[k];
                 double *X = which ? sV : sA;
                 const double xp = X[i * LD + p], xq = X[i * LD + q];
-                X[i * LD + p] = c * xp - s * xq;
-                X[i * LD + q] = s * xp + c * xq;
+                X[i * LD + p] = c * xp - sn * xq;
+                X[i * LD + q] = sn * xp + c * xq;
             }
             __syncthreads();
             // the rotated pair's off-diagonal entry is zero by construction: store it exactly
-            if (tid < half && cs_s[tid] != 0.0) {
+            if (tid < HALF && cs_s[tid] != 0.0) {
                 sA[cs_p[tid] * LD + cs_q[tid]] = 0.0;
                 sA[cs_q[tid] * LD + cs_p[tid]] = 0.0;
             }
@@ -123,7 +125,7 @@ __global__ void __launch_bounds__(BJ_THREADS)
     // rank the eigenvalues (ties broken by index) and write ascending eigenpairs
     double *ev = eval + (long long)blockIdx.x * n;
     double *V = evec + bofs;
-    for (int i = tid; i < n; i += BJ_THREADS) {
+    for (int i = tid; i < n; i += NT) {
         const double li = sA[i * LD + i];
         int rank = 0;
         for (int j = 0; j < n; ++j) {
@@ -133,6 +135,18 @@ __global__ void __launch_bounds__(BJ_THREADS)
         ev[rank] = li;
         for (int row = 0; row < n; ++row) V[row + (long long)rank * n] = sV[row * LD + i];
     }
+}
+
+template <int M, int NT>
+int launch_jacobi(const double *A, int n, int batch, double *eval, double *evec, int *status,
+                  cudaStream_t st) {
+    auto kern = batched_jacobi_kernel<M, NT>;
+    const size_t smem = sizeof(double) * 2 * (size_t)M * (M + 1);
+    CUEV_CHECK_STATUS(ensure_dyn_smem((const void *)kern, smem));
+    kern<<<batch, NT, smem, st>>>(A, n, eval, evec, status);
+    note_launch();
+    CUEV_TRY(cudaGetLastError());
+    return CUEV_OK;
 }
 
 // small per-device status buffer (one word per failure class); calls are serialised so that one
@@ -162,14 +176,15 @@ int batched_eigh_d(const double *A, int n, int batch, double *eval, double *evec
         if (!g_bj_status[dev]) CUEV_TRY(cudaMalloc(&g_bj_status[dev], DEV_STATUS_WORDS * sizeof(int)));
         status = g_bj_status[dev];
     }
-    const int m = n + (n & 1);
-    const size_t smem = sizeof(double) * 2 * (size_t)m * (m + 1);
-    CUEV_CHECK_STATUS(ensure_dyn_smem((const void *)batched_jacobi_kernel,
-                                      sizeof(double) * 2 * BJ_MAXN * (BJ_MAXN + 1)));
     CUEV_TRY(cudaMemsetAsync(status, 0, DEV_STATUS_WORDS * sizeof(int), st));
-    batched_jacobi_kernel<<<batch, BJ_THREADS, smem, st>>>(A, n, eval, evec, status);
-    note_launch();
-    CUEV_TRY(cudaGetLastError());
+    if (n <= 8)
+        CUEV_CHECK_STATUS((launch_jacobi<8, 32>(A, n, batch, eval, evec, status, st)));
+    else if (n <= 16)
+        CUEV_CHECK_STATUS((launch_jacobi<16, 64>(A, n, batch, eval, evec, status, st)));
+    else if (n <= 32)
+        CUEV_CHECK_STATUS((launch_jacobi<32, 256>(A, n, batch, eval, evec, status, st)));
+    else
+        CUEV_CHECK_STATUS((launch_jacobi<64, 256>(A, n, batch, eval, evec, status, st)));
     int host[DEV_STATUS_WORDS] = {0};
     CUEV_TRY(cudaMemcpyAsync(host, status, sizeof(host), cudaMemcpyDeviceToHost, st));
     CUEV_TRY(cudaStreamSynchronize(st));

@@ -19,6 +19,8 @@ struct cuev_handle_s {
 namespace cuev {
 namespace {
 
+thread_local double g_last_dc_flops = 0.0;
+
 struct CachedWs {
     Workspace *ws = nullptr;
     bool busy = false;
@@ -182,6 +184,8 @@ int solve_d(double *A, int n, double *eval, double *evec, cudaStream_t stream, c
     }
     CUEV_CHECK_STATUS(rec(5));
     CUEV_CHECK_STATUS(workspace_check_status(ws, "solve"));
+    if (evec) // the stream is synchronised: an 8-byte read for the profiling counter
+        CUEV_TRY(cudaMemcpy(&g_last_dc_flops, ws->dc_flops, sizeof(double), cudaMemcpyDeviceToHost));
     auto wall1 = std::chrono::high_resolution_clock::now();
     if (mixed && mixed->refine) {
         ws->mixed = 0;
@@ -281,6 +285,8 @@ extern "C" int cuev_ssyevd(float *A, int n, float *eval, float *evec, void *stre
     if (cudaStreamSynchronize(st) != cudaSuccess && s == CUEV_OK) s = CUEV_ERR_CUDA;
     return s;
 }
+
+extern "C" double cuev_last_dc_flops(void) { return cuev::g_last_dc_flops; }
 
 extern "C" int cuev_release_workspace(void) {
     std::lock_guard<std::mutex> lk(g_cache_mu);

@@ -35,6 +35,7 @@ struct Workspace {
     int *prog = nullptr;
     unsigned *bar = nullptr; // grid-barrier words for cooperative kernels
     int *status = nullptr;   // device status words (DEV_STATUS_WORDS ints)
+    double *dc_flops = nullptr; // flops of the D&C merge GEMMs of the last tridi_dc (after deflation)
     double *qr_part = nullptr;
     size_t qr_part_elems = 0;
     double *splitk = nullptr;

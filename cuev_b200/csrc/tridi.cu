@@ -594,8 +594,10 @@ __global__ void dc_svec_kernel(const MergeDesc *__restrict__ descs, int count, i
 }
 
 // GEMM descriptors: top rows use columns [0, ct1+ct2), bottom rows [ct1, ct1+ct2+ct3)
+// also counts the merge's GEMM flops, 2 (n1 k (ct1 + ct2) + n2 k (ct2 + ct3)), into *flops
 __global__ void dc_gemm_prep_kernel(const MergeDesc *__restrict__ descs, int count,
-                                    double *Q2, double *S, double *Out, GemmArgs *args, DcArrays a) {
+                                    double *Q2, double *S, double *Out, GemmArgs *args, DcArrays a,
+                                    double *flops) {
     const int mi = blockIdx.x * blockDim.x + threadIdx.x;
     if (mi >= count) return;
     const MergeDesc md = descs[mi];
@@ -622,6 +624,7 @@ __global__ void dc_gemm_prep_kernel(const MergeDesc *__restrict__ descs, int cou
     bot.C = Out + md.base + n1;
     args[2 * mi] = top;
     args[2 * mi + 1] = bot;
+    atomicAdd(flops, 2.0 * ((double)top.m * top.n * top.k + (double)bot.m * bot.n * bot.k));
 }
 
 // final order: roots (ascending) merged with the deflated eigenvalues (ranked here)
@@ -680,6 +683,7 @@ int tridi_dc(Workspace *ws, const double *d, const double *e, double *eval, doub
     const int n = ws->n;
     cudaStream_t st = ws->stream;
     if (n <= 0) return CUEV_OK;
+    CUEV_TRY(cudaMemsetAsync(ws->dc_flops, 0, sizeof(double), st));
     const long long ldq = n;
 
     // device scratch carve-up
@@ -770,7 +774,7 @@ int tridi_dc(Workspace *ws, const double *d, const double *e, double *eval, doub
         dc_svec_kernel<<<div_up(n * 32, 256), 256, 0, st>>>(dd, cnt, n, Dl, S, a); note_launch();
         // Delta is dead now: the GEMM output goes to its region
         dc_gemm_prep_kernel<<<div_up(cnt, 128), 128, 0, st>>>(dd, cnt, Q2, S, Dl, ws->dc_gemm_args,
-                                                              a); note_launch();
+                                                              a, ws->dc_flops); note_launch();
         CUEV_TRY(cudaGetLastError());
         CUEV_CHECK_STATUS(gemm_batched_launch(ws->dc_gemm_args, 2 * cnt, lvl_maxm[li], maxnm, 0, 0,
                                               st));

@@ -62,6 +62,7 @@ int workspace_create(int n, int b, int k, cudaStream_t stream, Workspace **out) 
         {(void **)&ws->prog, N * sizeof(int)},
         {(void **)&ws->bar, 64},
         {(void **)&ws->status, DEV_STATUS_WORDS * sizeof(int)},
+        {(void **)&ws->dc_flops, sizeof(double)},
         {(void **)&ws->qr_part, ws->qr_part_elems * s},
         {(void **)&ws->splitk, ws->splitk_bytes},
         {(void **)&ws->dc_vec, ws->dc_vec_elems * s},

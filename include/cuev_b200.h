@@ -162,6 +162,12 @@ const char *cuev_last_error(void);
 /* Number of CUDA kernels this library has launched since it was loaded (profiling aid). */
 long long cuev_kernel_launches(void);
 
+/* Flops of the divide-and-conquer merge GEMMs of the last full solve (with eigenvectors) on this
+ * host thread, counted on the device after deflation: sum over merges of
+ * 2 (n1 k (ct1 + ct2) + n2 k (ct2 + ct3)) (profiling aid; the upper bound without deflation is
+ * 4/3 n^3). */
+double cuev_last_dc_flops(void);
+
 /* Failure-path testing (no reference counterpart; the reference has no bounded waits).  Every
  * device-side wait of the library (bulge-chase hand-off, grid barriers, BC-back's warp pipeline,
  * the tensor-core GEMM's mbarriers) gives up after 2 s and the call returns CUEV_ERR_TIMEOUT.

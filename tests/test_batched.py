@@ -29,7 +29,7 @@ def test_oracle_batched_symmetrises_lower():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("n", [1, 2, 3, 5, 16, 31, 32, 33, 64])
+@pytest.mark.parametrize("n", [1, 2, 3, 5, 8, 9, 16, 17, 31, 32, 33, 64])
 def test_batched_random(cuda, n):
     import torch
     import cuev_b200 as cv
