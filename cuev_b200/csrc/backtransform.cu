@@ -12,10 +12,10 @@
 // (|s - s'| < b) or h' = h + 1 (s - s' < 2b); in both cases the true reverse order and this
 // order both apply (s, h) first, so the result is identical.  The payoff: block h+1 shares only
 // TS-1 rows with block h, so a thread can own one column of M and march down it with a register
-// window of TS+b-1 rows, applying TS reflectors per step with compile-time register indices and
-// reading w from shared memory as warp-wide broadcasts.  Columns are independent, so there is
-// no inter-thread communication at all.  (The reference slides a 256-row window per warp with
-// cross-lane shuffles and only supports b = 32, backtransform.cu:16,35.)
+// window of TS+b rows, applying TS reflectors per step with compile-time register indices and
+// reading w from shared memory as warp-wide broadcasts; the warps of a CTA run consecutive tiles
+// as a pipeline (below).  b = 32 and b = 64 both run it.  (The reference slides a 256-row
+// window per warp with cross-lane shuffles and only supports b = 32, backtransform.cu:16,35.)
 //
 // SBR-Back (M <- Q_s M).  Q_s = prod_j (I - Y_j T_j Y_j^T).  The reference applies each b-wide
 // panel with two K = b GEMMs (backtransform.cu:210-230).  Here the panels of one DBBR k-block are
@@ -45,155 +45,8 @@ __device__ __forceinline__ double2 lds2(const double *p) {
     return *reinterpret_cast<const double2 *>(p);
 }
 
-// One thread = one column of M; NWARP warps per CTA.  Shared memory (doubles):
-//   sW  [2][TS][BW]       static: reflectors of the current and the next hop block (cp.async)
-//   sIn [NT][BW+2]        dynamic: incoming rows of M for the next step (cp.async, coalesced)
-//   sOut[NT][BW+2]        dynamic: finished rows of M, stored cooperatively (coalesced)
-// The register window m[] is only ever indexed with compile-time constants and only exchanges
-// data with shared memory, which keeps it at 95 doubles without spills.
-template <int BW, int TS> constexpr size_t bc_back_smem(int nt) {
-    return sizeof(double) * (2 * (size_t)nt * (BW + 2));
-}
-
-template <int BW, int TS, int NWARP>
-__global__ void __launch_bounds__(32 * NWARP)
-    bc_back_kernel(const double *__restrict__ U, long long ldu, double *__restrict__ M,
-                   long long ldm, int n, int ncols) {
-    constexpr int NT = 32 * NWARP;
-    constexpr int R = TS + BW - 1; // register rows per column
-    constexpr int KEEP = TS - 1;   // rows carried from one hop block to the next
-    constexpr int MLD = BW + 2;    // 16-byte multiple, conflict-free 16-byte accesses
-    // reflectors in a static array: with an extern (dynamic) base the compiler spills the window
-    __shared__ __align__(16) double sW[2 * TS * BW];
-    extern __shared__ __align__(16) double bsm[];
-    double *sIn = bsm;
-    double *sOut = bsm + NT * MLD;
-    const int tid = threadIdx.x;
-    const int col0 = blockIdx.x * NT;
-    const int nsweeps = n - 2;
-    if (nsweeps <= 0) return;
-
-    // reflectors (s0 + t, h): rows [base + t, base + t + BW) of U[:, s0 + t]
-    auto stage_w = [&](int buf, int s0, int base) {
-        double *dst = sW + buf * TS * BW;
-#pragma unroll 4
-        for (int idx = tid; idx < TS * BW; idx += NT) {
-            const int t = idx / BW, i = idx % BW;
-            const int s = s0 + t, row = base + t + i;
-            const bool ok = (s < nsweeps) && (row < n);
-            cp_async8(dst + idx, ok ? U + row + (long long)s * ldu : U, ok);
-        }
-    };
-    // rows [row0, row0 + BW) of the CTA's columns -> sIn, coalesced along rows
-    auto stage_in = [&](int row0) {
-#pragma unroll 4
-        for (int idx = tid; idx < NT * BW; idx += NT) {
-            const int i = idx % BW, c = idx / BW;
-            const int row = row0 + i, cc = col0 + c;
-            const bool ok = (cc < ncols) && (row < n);
-            cp_async8(sIn + c * MLD + i, ok ? M + row + (long long)cc * ldm : M, ok);
-        }
-    };
-    // sOut -> rows [row0, row0 + cnt) of the CTA's columns
-    auto store_out = [&](int row0, int cnt) {
-        for (int idx = tid; idx < NT * BW; idx += NT) {
-            const int i = idx % BW, c = idx / BW;
-            const int row = row0 + i, cc = col0 + c;
-            if (i < cnt && cc < ncols && row < n) M[row + (long long)cc * ldm] = sOut[c * MLD + i];
-        }
-    };
-
-    double m[R];
-    const int ntile = (nsweeps + TS - 1) / TS;
-    const int mycol = min(col0 + tid, ncols - 1); // clamped: out-of-range lanes compute garbage
-    const bool active = col0 + tid < ncols;      // ... and never store it
-    const double *Mc = M + (long long)mycol * ldm;
-    for (int tile = ntile - 1; tile >= 0; --tile) {
-        const int s0 = tile * TS;
-        const int top = s0 + 1;              // first row touched by the tile
-        const int hmax = (n - 1 - top) / BW; // last hop block with rows inside the matrix
-        __syncthreads();
-        stage_w(0, s0, top);
-        stage_in(top + KEEP);
-        cp_async_commit();
-        // carried rows of the first step: [top, top + KEEP), rows past n read as 0
-#pragma unroll
-        for (int i = 0; i < KEEP; ++i) {
-            const int row = top + i;
-            const double v = Mc[min(row, n - 1)];
-            m[i] = row < n ? v : 0.0;
-        }
-        for (int h = 0; h <= hmax; ++h) {
-            const int base = top + h * BW; // row of m[0]
-            cp_async_wait<0>();
-            __syncthreads(); // sW[h & 1] and sIn complete; previous sOut stored
-#pragma unroll
-            for (int i = 0; i < BW; ++i) m[KEEP + i] = sIn[tid * MLD + i];
-            __syncthreads(); // everyone has read sIn
-            if (h < hmax) {
-                stage_w((h + 1) & 1, s0, base + BW);
-                stage_in(base + BW + KEEP);
-            }
-            cp_async_commit();
-            const double *W = sW + (h & 1) * TS * BW;
-            // apply in decreasing sweep order: m[t : t+BW] -= 2 (w^T m) w
-#pragma unroll
-            for (int t = TS - 1; t >= 0; --t) {
-                const double *w = W + t * BW;
-                double acc[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-#pragma unroll
-                for (int i = 0; i < BW; i += 2) {
-                    // compiler-only fence every 32 entries: keeps at most 32 w values in flight
-                    if (i % 32 == 0) asm volatile("" ::: "memory");
-                    const double2 ww = lds2(w + i);
-                    acc[(i >> 1) & 3] = fma(ww.x, m[t + i], acc[(i >> 1) & 3]);
-                    acc[4 + ((i >> 1) & 3)] = fma(ww.y, m[t + i + 1], acc[4 + ((i >> 1) & 3)]);
-                }
-                const double f =
-                    -2.0 * (((acc[0] + acc[1]) + (acc[2] + acc[3])) +
-                            ((acc[4] + acc[5]) + (acc[6] + acc[7])));
-#pragma unroll
-                for (int i = 0; i < BW; i += 2) {
-                    if (i % 32 == 0) asm volatile("" ::: "memory");
-                    const double2 ww = lds2(w + i);
-                    m[t + i] = fma(f, ww.x, m[t + i]);
-                    m[t + i + 1] = fma(f, ww.y, m[t + i + 1]);
-                }
-            }
-            // rows [base, base + BW) are final for this tile; carry the rest down
-#pragma unroll
-            for (int i = 0; i < BW; ++i) sOut[tid * MLD + i] = m[i];
-#pragma unroll
-            for (int i = 0; i < KEEP; ++i) m[i] = m[i + BW];
-            __syncthreads();
-            store_out(base, BW);
-        }
-        // flush the carried rows [top + (hmax+1) BW, ... + KEEP)
-        const int fbase = top + (hmax + 1) * BW;
-        if (active) {
-            double *Mw = M + (long long)mycol * ldm;
-#pragma unroll
-            for (int i = 0; i < KEEP; ++i)
-                if (fbase + i < n) Mw[fbase + i] = m[i];
-        }
-    }
-}
-
-template <int BW, int TS> int launch_bc_back(Workspace *ws, double *M, long long ldm, int ncols) {
-    constexpr int NWARP = 2;
-    constexpr int NT = 32 * NWARP;
-    const size_t smem = bc_back_smem<BW, TS>(NT);
-    auto kern = bc_back_kernel<BW, TS, NWARP>;
-    CUEV_CHECK_STATUS(ensure_dyn_smem((const void *)kern, smem));
-    const int grid = div_up(ncols, NT);
-    kern<<<grid, NT, smem, ws->stream>>>(ws->U, ws->n, M, ldm, ws->n, ncols); note_launch();
-    CUEV_TRY(cudaGetLastError());
-    return CUEV_OK;
-}
-
-
 // ---------------------------------------------------------------------------------------------
-// Pipelined BC-Back for b = 32.
+// Pipelined BC-Back (b = PB = 32 or 64; written for 32 below, the same with 64-row chunks).
 //
 // The one-thread-per-column kernel above has only n threads of parallelism (n/32 warps: about
 // 3.5 warps per SM at n = 16384), far too few to hide FP64 and shared-memory latency.  Here a
@@ -210,14 +63,20 @@ template <int BW, int TS> int launch_bc_back(Workspace *ws, double *M, long long
 // per round of P tiles.  Every wait is on a shared-memory counter, bounded by time, and all the
 // warps that wait on one another belong to one CTA (so they are co-resident).
 //
-// Per hop a warp applies TS reflectors of length 32 to its 32 columns: the reflector is loaded
-// once from shared memory (16 broadcast 16-byte loads) into registers and used for both the dot
-// product and the update, 64 FMAs per lane per reflector.
-constexpr int PB = 32;
-
-template <int TS, int P> struct PipeSmem {
+// Per hop a warp applies TS reflectors of length PB to its 32 columns.  At PB = 32 the reflector
+// is loaded once from shared memory (16 broadcast 16-byte loads) into registers and used for both
+// the dot product and the update, 64 FMAs per lane per reflector.  At PB = 64 the 80-row window
+// and a 64-entry reflector do not both fit the registers: the reflector is read from shared
+// memory for the dot product and again for the update (broadcast loads), 128 FMAs per lane; the
+// shared memory then holds four warps (one CTA of 128 threads per SM).
+// Why the chunking is exact for any b: tile t-1's window at hop h is rows
+// [top_t - TS + h b, top_t + h b + b), whose incoming rows [top_t + h b, + b) are tile t's chunk h,
+// final for tile t once its hop h is done; and a reflector (s', h') of tile t - 1 commutes with
+// every (s, h'') of tile t with h'' >= h' + 1 (their rows are disjoint), so running tile t - 1 one
+// hop block behind tile t applies the reflectors in an order equivalent to the reverse order.
+template <int TS, int P, int PB> struct PipeSmem {
     double w[P][2][TS][PB];        // reflectors of each warp's current and next hop block
-    double ring[P - 1][2][PB][32]; // warp p -> warp p+1, two chunks of 32 rows x 32 columns
+    double ring[P - 1][2][PB][32]; // warp p -> warp p+1, two chunks of PB rows x 32 columns
     double xin[2][PB][32];         // warp 0: incoming rows (from X or, first tile, from M)
     int prod[P], cons[P];          // ring p: chunks written / chunks fully read (monotonic)
     int gprog;                     // chunks the last warp has written to X (monotonic)
@@ -263,14 +122,15 @@ __device__ __forceinline__ bool pipe_wait(const int *flag, int target, int *abor
     }
 }
 
-template <int TS, int P>
+template <int TS, int P, int PB>
 __global__ void __launch_bounds__(32 * P, 1)
     bc_back_pipe_kernel(const double *__restrict__ U, long long ldu, double *__restrict__ M,
                         long long ldm, double *__restrict__ X, int n, int ncols,
                         int *__restrict__ status) {
+    static_assert(PB == 32 || PB == 64, "band width 32 or 64");
     constexpr int R = TS + PB; // register window rows
     extern __shared__ __align__(16) unsigned char pipe_smem_raw[];
-    PipeSmem<TS, P> &S = *reinterpret_cast<PipeSmem<TS, P> *>(pipe_smem_raw);
+    PipeSmem<TS, P, PB> &S = *reinterpret_cast<PipeSmem<TS, P, PB> *>(pipe_smem_raw);
     const int lane = threadIdx.x & 31, p = threadIdx.x >> 5;
     const int col0 = blockIdx.x * 32;
     const int mycol = min(col0 + lane, ncols - 1); // clamped: lanes past ncols never store to M
@@ -283,19 +143,23 @@ __global__ void __launch_bounds__(32 * P, 1)
     if (threadIdx.x == 0) S.gprog = 0, S.abort_flag = 0;
     __syncthreads(); // the only CTA-wide barrier: warps leave at different times
 
-    // reflectors (s0 + j, hop of `rbase`): rows [rbase + j, rbase + j + 32) of U[:, s0 + j]
+    // reflectors (s0 + j, hop of `rbase`): rows [rbase + j, rbase + j + PB) of U[:, s0 + j]
     auto stage_w = [&](int buf, int s0, int rbase) {
 #pragma unroll
         for (int j = 0; j < TS; ++j) {
-            const int s = s0 + j, row = rbase + j + lane;
-            const bool ok = (s < nsweeps) && (row < n);
-            cp_async8(&S.w[p][buf][j][lane], ok ? U + row + (long long)s * ldu : U, ok);
+#pragma unroll
+            for (int t = 0; t < PB / 32; ++t) {
+                const int s = s0 + j, row = rbase + j + lane + 32 * t;
+                const bool ok = (s < nsweeps) && (row < n);
+                cp_async8(&S.w[p][buf][j][lane + 32 * t], ok ? U + row + (long long)s * ldu : U,
+                          ok);
+            }
         }
     };
-    // warp 0's incoming chunk: 32 rows from X (coalesced 16-byte copies) ...
+    // warp 0's incoming chunk: PB rows from X (coalesced 16-byte copies) ...
     auto stage_x = [&](int buf, int row0) {
 #pragma unroll
-        for (int q = 0; q < 16; ++q) {
+        for (int q = 0; q < PB / 2; ++q) {
             const int e = q * 64 + lane * 2; // element pair (row e / 32, columns e % 32, +1)
             const int r = row0 + (e >> 5);
             const bool ok = r < n;
@@ -393,26 +257,57 @@ __global__ void __launch_bounds__(32 * P, 1)
 
             // apply the tile's reflectors of this hop, last sweep first
             const double *W = &S.w[p][h & 1][0][0];
+            if constexpr (PB == 32) {
 #pragma unroll
-            for (int j = TS - 1; j >= 0; --j) {
-                double wr[PB];
+                for (int j = TS - 1; j >= 0; --j) {
+                    double wr[PB];
 #pragma unroll
-                for (int i = 0; i < PB; i += 2) {
-                    const double2 v = lds2(W + j * PB + i);
-                    wr[i] = v.x, wr[i + 1] = v.y;
+                    for (int i = 0; i < PB; i += 2) {
+                        const double2 v = lds2(W + j * PB + i);
+                        wr[i] = v.x, wr[i + 1] = v.y;
+                    }
+                    double acc[8];
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) acc[i] = wr[i] * m[j + i];
+#pragma unroll
+                    for (int i = 8; i < PB; ++i) acc[i & 7] = fma(wr[i], m[j + i], acc[i & 7]);
+                    const double f = -2.0 * (((acc[0] + acc[1]) + (acc[2] + acc[3])) +
+                                             ((acc[4] + acc[5]) + (acc[6] + acc[7])));
+#pragma unroll
+                    for (int i = 0; i < PB; ++i) m[j + i] = fma(f, wr[i], m[j + i]);
                 }
-                double acc[8];
+            } else {
 #pragma unroll
-                for (int i = 0; i < 8; ++i) acc[i] = wr[i] * m[j + i];
+                for (int j = TS - 1; j >= 0; --j) {
+                    const double *Wj = W + j * PB;
+                    double acc[8];
+                    // keep each phase's reflector loads inside the phase: hoisted across
+                    // reflectors they outgrow the registers the window leaves
+                    asm volatile("" ::: "memory");
 #pragma unroll
-                for (int i = 8; i < PB; ++i) acc[i & 7] = fma(wr[i], m[j + i], acc[i & 7]);
-                const double f = -2.0 * (((acc[0] + acc[1]) + (acc[2] + acc[3])) +
-                                         ((acc[4] + acc[5]) + (acc[6] + acc[7])));
+                    for (int i = 0; i < PB; i += 2) {
+                        const double2 v = lds2(Wj + i);
+                        if (i < 8) {
+                            acc[i] = v.x * m[j + i];
+                            acc[i + 1] = v.y * m[j + i + 1];
+                        } else {
+                            acc[i & 7] = fma(v.x, m[j + i], acc[i & 7]);
+                            acc[(i + 1) & 7] = fma(v.y, m[j + i + 1], acc[(i + 1) & 7]);
+                        }
+                    }
+                    const double f = -2.0 * (((acc[0] + acc[1]) + (acc[2] + acc[3])) +
+                                             ((acc[4] + acc[5]) + (acc[6] + acc[7])));
+                    asm volatile("" ::: "memory");
 #pragma unroll
-                for (int i = 0; i < PB; ++i) m[j + i] = fma(f, wr[i], m[j + i]);
+                    for (int i = 0; i < PB; i += 2) {
+                        const double2 v = lds2(Wj + i);
+                        m[j + i] = fma(f, v.x, m[j + i]);
+                        m[j + i + 1] = fma(f, v.y, m[j + i + 1]);
+                    }
+                }
             }
 
-            // rows [base, base + 32) are final for this tile
+            // rows [base, base + PB) are final for this tile
             if (to_m) {
                 if (active) {
                     double *Mw = M + (long long)mycol * ldm;
@@ -456,13 +351,13 @@ __global__ void __launch_bounds__(32 * P, 1)
 // Columns [c0, c0 + ncols) of M (c0 a multiple of 32): CTA g owns columns c0 + 32 g .. + 31 and
 // its hand-off rows in dc_S at the offset of its 32-column group, so launches over disjoint
 // column ranges are independent and together do what one launch over all columns does.
-template <int TS, int P>
+template <int TS, int P, int PB>
 int launch_bc_back_pipe(Workspace *ws, cudaStream_t st, double *M, long long ldm, int c0,
                         int ncols) {
     const int n = ws->n;
     if (ncols <= 0) return CUEV_OK;
-    const size_t smem = sizeof(PipeSmem<TS, P>);
-    auto kern = bc_back_pipe_kernel<TS, P>;
+    const size_t smem = sizeof(PipeSmem<TS, P, PB>);
+    auto kern = bc_back_pipe_kernel<TS, P, PB>;
     CUEV_CHECK_STATUS(ensure_dyn_smem((const void *)kern, smem));
     const int grid = div_up(ncols, 32);
     double *Xc = ws->dc_S + (size_t)(c0 / 32) * n * 32;
@@ -483,6 +378,16 @@ int bt_gemm(Workspace *ws, int ta, int tb, int m, int n, int k, double alpha, co
         return i8_dgemm(ta, tb, 0, m, n, k, MIXED_SLICES, alpha, A, lda, B, ldb, beta, C, ldc, 0,
                         ws->i8_scratch, ws->status, ws->stream);
     return ws_gemm(ws, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+}
+
+// BC-back over columns [c0, c0 + ncols): b = 32 runs 8 warps on 16-sweep tiles (79-row register
+// window, 252 registers); b = 64 runs 4 warps on 16-sweep tiles (80-row window, the reflector
+// streamed from shared memory), which is what fits 227 KB of shared memory with two-chunk rings.
+int launch_bc_back_cols(Workspace *ws, cudaStream_t st, double *M, long long ldm, int c0,
+                        int ncols) {
+    if (ws->b == 32) return launch_bc_back_pipe<16, 8, 32>(ws, st, M, ldm, c0, ncols);
+    if (ws->b == 64) return launch_bc_back_pipe<8, 4, 64>(ws, st, M, ldm, c0, ncols);
+    return CUEV_ERR_INVALID;
 }
 
 // M <- Q_s M on ncols columns of M, with X (w x ncols) and X2 (w x ncols) as scratch.
@@ -513,11 +418,7 @@ int sbr_back_cols(Workspace *ws, double *M, long long ldm, int ncols, double *X,
 
 int bc_back(Workspace *ws, double *M, long long ldm) {
     if (ws->n <= 2) return CUEV_OK;
-    // register window R = TS + b - 1 rows: 79 rows keeps b = 32 spill-free (252 registers);
-    // b = 64 needs the 64 reflector entries live as well and runs a shorter tile
-    if (ws->b == 32) return launch_bc_back_pipe<16, 8>(ws, ws->stream, M, ldm, 0, ws->n);
-    if (ws->b == 64) return launch_bc_back<64, 16>(ws, M, ldm, ws->n);
-    return CUEV_ERR_INVALID;
+    return launch_bc_back_cols(ws, ws->stream, M, ldm, 0, ws->n);
 }
 
 int sbr_back(Workspace *ws, double *M, long long ldm) {
@@ -536,16 +437,16 @@ int back_transform(Workspace *ws, double *M, long long ldm, cudaEvent_t bc_end) 
     const int n = ws->n;
     const int groups = div_up(std::max(n, 1), 32);
     const int full = groups / num_sms() * num_sms(); // groups in whole waves
-    if (ws->b != 32 || n <= 2 || full == 0 || full == groups || !ws->side) {
+    if (n <= 2 || full == 0 || full == groups || !ws->side) {
         CUEV_CHECK_STATUS(bc_back(ws, M, ldm));
         if (bc_end) CUEV_TRY(cudaEventRecord(bc_end, ws->stream));
         return sbr_back(ws, M, ldm);
     }
     const int c1 = full * 32;
-    CUEV_CHECK_STATUS((launch_bc_back_pipe<16, 8>(ws, ws->stream, M, ldm, 0, c1)));
+    CUEV_CHECK_STATUS(launch_bc_back_cols(ws, ws->stream, M, ldm, 0, c1));
     CUEV_TRY(cudaEventRecord(ws->ev_a, ws->stream));
     CUEV_TRY(cudaStreamWaitEvent(ws->side, ws->ev_a, 0));
-    int st = launch_bc_back_pipe<16, 8>(ws, ws->side, M, ldm, c1, n - c1);
+    int st = launch_bc_back_cols(ws, ws->side, M, ldm, c1, n - c1);
     if (st == CUEV_OK && bc_end && cudaEventRecord(bc_end, ws->side) != cudaSuccess)
         st = CUEV_ERR_CUDA;
     if (st == CUEV_OK && cudaEventRecord(ws->ev_b, ws->side) != cudaSuccess) st = CUEV_ERR_CUDA;
