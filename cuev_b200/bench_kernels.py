@@ -8,6 +8,7 @@
     python -m cuev_b200.bench_kernels refine N [--iters K]       Ogita-Aishima refinement
     python -m cuev_b200.bench_kernels eigvals N                  eigenvalues-only solve
     python -m cuev_b200.bench_kernels mixed N [--iters K]        precision form vs FP64 solve
+    python -m cuev_b200.bench_kernels overlap N                  D&C and BC-back alone / together
     python -m cuev_b200.bench_kernels adjoint N                  eigh forward + adjoint
     python -m cuev_b200.bench_kernels batched N BATCH            batched small-n eigh vs torch
 
@@ -148,6 +149,65 @@ def run_stages(a):
         return {"kernel": "stages", "n": n, "nbw": a.nbw, "nk": a.nk, "ms": out, **rates}
     finally:
         h.close()
+
+
+def run_overlap(a):
+    """How much of BC-back (FP64 FMA, one CTA per SM) can hide under the divide and conquer
+    (DMMA merge GEMMs and latency-bound kernels) when both run at once: the only gain open to a
+    reordered back-transform that applies Q_b while D&C runs.  Two handles on two streams, each
+    after its own band reduction and chase of the same matrix; times by CUDA events."""
+    n = a.M
+    A0 = _rand(n, n, 7)
+    A0 = ((A0 + A0.t()) * 0.5).contiguous()
+    s1, s2 = torch.cuda.Stream(), torch.cuda.Stream()
+    h1 = cv.SolverHandle(n, a.nbw, a.nk, stream=s1)
+    h2 = cv.SolverHandle(n, a.nbw, a.nk, stream=s2)
+    try:
+        b = a.nbw
+        vec = lambda: torch.empty(n, dtype=torch.float64, device="cuda")  # noqa: E731
+        d1, e1, w1, d2, e2 = vec(), vec(), vec(), vec(), vec()
+        Q1 = torch.empty(n, n, dtype=torch.float64, device="cuda")
+        M2 = _rand(n, n, 11)
+        for h, st, d, e in ((h1, s1, d1, e1), (h2, s2, d2, e2)):
+            A = A0.clone()
+            with torch.cuda.stream(st):
+                h.dbbr_reduce(A)
+                Bt, _ = h.buffer(cv.BUF_B, 2 * b, n)
+                h.bc_chase(Bt, d, e)
+            torch.cuda.synchronize()
+            del A, Bt
+        res = {"dc": [], "bc_back": [], "together": []}
+        for rep in range(a.warmup + a.reps):
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
+            # alone
+            ev[0].record(s1)
+            h1.tridi_dc(d1, e1, w1, Q1)
+            ev[1].record(s1)
+            torch.cuda.synchronize()
+            ev[2].record(s2)
+            h2.bc_back(M2, n)
+            ev[3].record(s2)
+            torch.cuda.synchronize()
+            # together: both streams start at one event
+            ev[4].record(s1)
+            s2.wait_event(ev[4])
+            h2.bc_back(M2, n)
+            e_b = torch.cuda.Event(enable_timing=True)
+            e_b.record(s2)
+            h1.tridi_dc(d1, e1, w1, Q1)
+            s1.wait_event(e_b)
+            ev[5].record(s1)
+            torch.cuda.synchronize()
+            if rep >= a.warmup:
+                res["dc"].append(ev[0].elapsed_time(ev[1]))
+                res["bc_back"].append(ev[2].elapsed_time(ev[3]))
+                res["together"].append(ev[4].elapsed_time(ev[5]))
+        out = {k: round(statistics.median(v), 2) for k, v in res.items()}
+        out["hidden_ms"] = round(out["dc"] + out["bc_back"] - out["together"], 2)
+        return {"kernel": "overlap_dc_bc_back", "n": n, "nbw": a.nbw, "nk": a.nk, **out}
+    finally:
+        h1.close()
+        h2.close()
 
 
 def run_refine(a):
@@ -320,7 +380,7 @@ def run_batched(a):
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("what", choices=["gemm", "i8gemm", "symm", "syr2k", "stages", "refine",
-                                     "eigvals", "adjoint", "batched", "mixed"])
+                                     "eigvals", "adjoint", "batched", "mixed", "overlap"])
     ap.add_argument("M", type=int)
     ap.add_argument("N", type=int, nargs="?", default=0)
     ap.add_argument("K", type=int, nargs="?", default=0)
@@ -333,11 +393,11 @@ def main(argv=None):
     ap.add_argument("--reps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=2)
     a = ap.parse_args(argv)
-    if a.what in ("stages", "eigvals", "adjoint") and a.nk == 0:
+    if a.what in ("stages", "eigvals", "adjoint", "overlap") and a.nk == 0:
         a.nk = 512 if a.M >= 8192 else 256
     fn = {"gemm": run_gemm, "i8gemm": run_i8gemm, "symm": run_symm, "syr2k": run_syr2k, "stages": run_stages,
           "refine": run_refine, "eigvals": run_eigvals, "adjoint": run_adjoint,
-          "batched": run_batched, "mixed": run_mixed}[a.what]
+          "batched": run_batched, "mixed": run_mixed, "overlap": run_overlap}[a.what]
     print(json.dumps(fn(a)), flush=True)
 
 

@@ -168,12 +168,19 @@ __global__ void __launch_bounds__(32 * P, 1)
         }
     };
     // ... or, for the first tile, from M (one column per lane)
+    // (full chunks take an unpredicated path: per-row predicates on the 64-row chunks of b = 64
+    // cost registers the window needs)
     auto stage_m = [&](int buf, int row0) {
+        if (row0 + PB <= n) {
 #pragma unroll
-        for (int i = 0; i < PB; ++i) {
-            const int r = row0 + i;
-            const bool ok = r < n;
-            cp_async8(&S.xin[buf][i][lane], ok ? Mc + r : Mc, ok);
+            for (int i = 0; i < PB; ++i) cp_async8(&S.xin[buf][i][lane], Mc + row0 + i, true);
+        } else {
+#pragma unroll
+            for (int i = 0; i < PB; ++i) {
+                const int r = row0 + i;
+                const bool ok = r < n;
+                cp_async8(&S.xin[buf][i][lane], ok ? Mc + r : Mc, ok);
+            }
         }
     };
 
@@ -281,9 +288,6 @@ __global__ void __launch_bounds__(32 * P, 1)
                 for (int j = TS - 1; j >= 0; --j) {
                     const double *Wj = W + j * PB;
                     double acc[8];
-                    // keep each phase's reflector loads inside the phase: hoisted across
-                    // reflectors they outgrow the registers the window leaves
-                    asm volatile("" ::: "memory");
 #pragma unroll
                     for (int i = 0; i < PB; i += 2) {
                         const double2 v = lds2(Wj + i);
@@ -297,7 +301,6 @@ __global__ void __launch_bounds__(32 * P, 1)
                     }
                     const double f = -2.0 * (((acc[0] + acc[1]) + (acc[2] + acc[3])) +
                                              ((acc[4] + acc[5]) + (acc[6] + acc[7])));
-                    asm volatile("" ::: "memory");
 #pragma unroll
                     for (int i = 0; i < PB; i += 2) {
                         const double2 v = lds2(Wj + i);
@@ -310,15 +313,26 @@ __global__ void __launch_bounds__(32 * P, 1)
             // rows [base, base + PB) are final for this tile
             if (to_m) {
                 if (active) {
-                    double *Mw = M + (long long)mycol * ldm;
+                    double *Mw = M + (long long)mycol * ldm + base;
+                    if (base + PB <= n) {
 #pragma unroll
-                    for (int i = 0; i < PB; ++i)
-                        if (base + i < n) Mw[base + i] = m[i];
+                        for (int i = 0; i < PB; ++i) Mw[i] = m[i];
+                    } else {
+#pragma unroll
+                        for (int i = 0; i < PB; ++i)
+                            if (base + i < n) Mw[i] = m[i];
+                    }
                 }
             } else if (to_x) {
+                double *Xr = Xg + (size_t)base * 32 + lane;
+                if (base + PB <= n) {
 #pragma unroll
-                for (int i = 0; i < PB; ++i)
-                    if (base + i < n) __stcg(Xg + (size_t)(base + i) * 32 + lane, m[i]);
+                    for (int i = 0; i < PB; ++i) __stcg(Xr + 32 * i, m[i]);
+                } else {
+#pragma unroll
+                    for (int i = 0; i < PB; ++i)
+                        if (base + i < n) __stcg(Xr + 32 * i, m[i]);
+                }
                 ++oseq;
                 // The first warp of the next round reads these rows almost a whole tile later,
                 // so the device-scope fence (the costliest step of a hop) is paid once per 8 hops
