@@ -129,7 +129,7 @@ typedef enum cuev_products {
 int cuev_dsyev_refine_ex(const double *A, int n, double *eval, double *evec, int max_iters,
                          double tol, int products, void *stream, cuev_refine_info *info);
 
-/* Precision form (no reference counterpart; the north star's mixed+refine solve).  Same
+/* Precision form (no reference counterpart): a mixed-precision solve refined to FP64.  Same
  * arguments and result as cuev_dsyevd (A overwritten, eval ascending, evec columns), computed
  * in two parts:
  *   1. a first solve whose back-transform products Y^T M, T X and Y X (SBR-back, each of at
