@@ -253,7 +253,7 @@ def eigvalsh(A_rowmajor_sym, nbw: int = 0, nk: int = 0):
 
 
 def eigh_batched(A_batch):
-    """Eigen-decompositions of a stack of small symmetric matrices (batch, n, n), n <= 64, in one
+    """Eigen-decompositions of a stack of small symmetric matrices (batch, n, n), n <= 512, in one
     launch.  Returns (w, V) with A[b] = V[b] diag(w[b]) V[b]^T; reads the lower triangles."""
     import torch
     if A_batch.dim() != 3 or A_batch.shape[1] != A_batch.shape[2]:

@@ -1,6 +1,7 @@
-// Batched eigensolver for many small symmetric matrices (n <= 64), one CTA per matrix: the
-// "batched small-n eigh" path for framework wrappers that carry stacks of small problems.  The
-// reference has no batched entry (its solve takes one matrix).
+// Batched eigensolver for many small symmetric matrices (n <= 64 here; 64 < n <= 512 in
+// batched_mid.cu), one CTA per matrix: the "batched small-n eigh" path for framework wrappers that
+// carry stacks of small problems.  The reference has no batched entry (its solve takes one
+// matrix).
 //
 // Method: two-sided cyclic Jacobi with the round-robin (tournament) ordering, so each round
 // rotates n/2 disjoint index pairs at once.  For a pair (p, q) the rotation is the symmetric
@@ -28,6 +29,7 @@ namespace cuev {
 namespace {
 
 constexpr int BJ_MAXN = 64;
+constexpr int BMID_MAXN = 512;
 constexpr int BJ_MAX_SWEEPS = 60;
 
 template <int M, int NT>
@@ -157,13 +159,17 @@ int *g_bj_status[64] = {nullptr};
 
 } // namespace
 
+// 64 < n <= 512: Householder tridiagonalisation + implicit QL, one CTA per matrix (batched_mid.cu)
+int batched_eigh_mid(const double *A, int n, int batch, double *eval, double *evec, int *status,
+                     cudaStream_t st);
+
 int batched_eigh_d(const double *A, int n, int batch, double *eval, double *evec,
                    cudaStream_t st) {
     if (n < 0 || batch < 0) return CUEV_ERR_INVALID;
     if (n == 0 || batch == 0) return CUEV_OK;
     if (!A || !eval || !evec) return CUEV_ERR_INVALID;
-    if (n > BJ_MAXN) {
-        set_last_message("batched eigensolver: n > 64 (use the full solver per matrix)");
+    if (n > BMID_MAXN) {
+        set_last_message("batched eigensolver: n > 512 (use the full solver per matrix)");
         return CUEV_ERR_UNSUPPORTED;
     }
     int dev = 0;
@@ -183,15 +189,21 @@ int batched_eigh_d(const double *A, int n, int batch, double *eval, double *evec
         CUEV_CHECK_STATUS((launch_jacobi<16, 64>(A, n, batch, eval, evec, status, st)));
     else if (n <= 32)
         CUEV_CHECK_STATUS((launch_jacobi<32, 256>(A, n, batch, eval, evec, status, st)));
-    else
+    else if (n <= BJ_MAXN)
         CUEV_CHECK_STATUS((launch_jacobi<64, 256>(A, n, batch, eval, evec, status, st)));
+    else
+        CUEV_CHECK_STATUS(batched_eigh_mid(A, n, batch, eval, evec, status, st));
     int host[DEV_STATUS_WORDS] = {0};
     CUEV_TRY(cudaMemcpyAsync(host, status, sizeof(host), cudaMemcpyDeviceToHost, st));
     CUEV_TRY(cudaStreamSynchronize(st));
     if (host[DEV_STATUS_CODE] != 0) {
         char msg[128];
-        snprintf(msg, sizeof(msg), "batched eigensolver: Jacobi did not converge (matrix %d)",
-                 host[DEV_STATUS_WHERE]);
+        if (host[DEV_STATUS_CODE] == CUEV_ERR_NONFINITE)
+            snprintf(msg, sizeof(msg), "batched eigensolver: NaN or Inf in matrix %d",
+                     host[DEV_STATUS_WHERE]);
+        else
+            snprintf(msg, sizeof(msg), "batched eigensolver: %s did not converge (matrix %d)",
+                     n <= BJ_MAXN ? "Jacobi" : "QL", host[DEV_STATUS_WHERE]);
         set_last_message(msg);
         return host[DEV_STATUS_CODE];
     }

@@ -288,7 +288,12 @@ extern "C" int cuev_ssyevd(float *A, int n, float *eval, float *evec, void *stre
 
 extern "C" double cuev_last_dc_flops(void) { return cuev::g_last_dc_flops; }
 
+namespace cuev {
+void batched_mid_release();
+}
+
 extern "C" int cuev_release_workspace(void) {
+    cuev::batched_mid_release();
     std::lock_guard<std::mutex> lk(g_cache_mu);
     for (auto &c : g_cache) {
         if (c.ws && !c.busy) {

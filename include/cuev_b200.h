@@ -80,11 +80,13 @@ int cuev_dsyevd_cfg(double *A, int n, double *eval, double *evec, void *stream, 
 int cuev_ssyevd(float *A, int n, float *eval, float *evec, void *stream, cuev_timer *timer);
 
 /* Batched eigensolver for many small matrices (no reference counterpart: the reference solves one
- * matrix per call).  A holds `batch` symmetric n x n matrices, n <= 64, each column-major and
+ * matrix per call).  A holds `batch` symmetric n x n matrices, n <= 512, each column-major and
  * stored one after another (stride n*n); only their lower triangles are read and A is not
  * modified.  eval receives batch x n ascending eigenvalues, evec batch x (n x n) eigenvector
- * columns.  One CTA per matrix (two-sided Jacobi in shared memory).  n > 64 returns
- * CUEV_ERR_UNSUPPORTED.  Blocks until done. */
+ * columns.  One CTA per matrix: two-sided Jacobi in shared memory for n <= 64; Householder
+ * tridiagonalisation, implicit QL and back-transform in a per-CTA device workspace (kept per
+ * device, 3 n^2 doubles per resident CTA) for 64 < n <= 512.  n > 512 returns
+ * CUEV_ERR_UNSUPPORTED.  Blocks until done; calls are serialised. */
 int cuev_dsyevd_batched(const double *A, int n, int batch, double *eval, double *evec,
                         void *stream);
 
@@ -153,7 +155,8 @@ int cuev_dsyevd_mixed(double *A, int n, double *eval, double *evec, void *stream
                       cuev_timer *timer, int max_refine_iters, double tol,
                       cuev_mixed_info *info);
 
-/* Release the cached device workspace (the solves keep one pool per (n, b, k) between calls). */
+/* Release the cached device workspace (the solves keep one pool per (n, b, k) between calls, the
+ * batched eigensolver one buffer per device for 64 < n <= 512). */
 int cuev_release_workspace(void);
 
 /* Message for the last failing call on this host thread ("" if none). */
