@@ -40,13 +40,16 @@ constexpr int PF = 8; // loads in flight per thread in the row passes
 // NT threads own rows t, t + NT, ... (R rows each) of matrices with n <= NT R; QL applies K
 // sweeps per pass over a row (prefetch distance QL_D, register window 2K + QL_D); the
 // back-transform takes BTK reflectors per block.  Shared memory is sized so that several CTAs
-// (and so several rotation generators) share an SM.
+// (and so several rotation generators) share an SM.  During QL the last warp only generates
+// rotations (lane 0) and the rows are spread over the other NT - 32 threads: a generating lane
+// in a warp that also applies rotations would serialise the warp's two paths.
 template <int NT_, int R_, int K_, int BTK_> struct MidCfg {
     static constexpr int NT = NT_, R = R_, K = K_, BTK = BTK_;
     static constexpr int MAXN = NT * R;
     static constexpr int QL_D = 8;
     static constexpr int QL_W = 2 * K + QL_D;
-    static constexpr int GEN = NT - 1; // the thread that generates the rotations
+    static constexpr int GEN = NT - 32;  // the thread that generates the rotations
+    static constexpr int NAPP = NT - 32; // the threads that apply them
     static_assert(NT % 32 == 0 && NT >= BTK && BTK % 2 == 0, "shape");
 };
 
@@ -718,7 +721,8 @@ __global__ void __launch_bounds__(C::NT, (65536 / 128) / C::NT)
                     if (sm.u.ql.cnt[buf] == 0) break; // uniform
                     if (t == C::GEN) ql_generate<C>(sm, buf ^ 1, n, q);
 #pragma unroll 1
-                    for (int r = t; r < n; r += NT) ql_apply_row<C>(Zc + r, n, sm, buf);
+                    for (int r = t; t < C::NAPP && r < n; r += C::NAPP)
+                        ql_apply_row<C>(Zc + r, n, sm, buf);
                     __syncthreads();
                 }
                 for (int r = t; r < n; r += NT) sm.d[r] /= sm.scale;
