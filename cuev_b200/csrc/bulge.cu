@@ -13,10 +13,14 @@
 //    ld.global.cg so no SM sees a stale L1 line of data another SM has just rewritten;
 //  * hand-off between sweeps is acquire/release on prog[] with a BOUNDED wait (the reference
 //    spins forever, bulge.cu:194-196); on timeout the kernel records CUEV_ERR_TIMEOUT and exits;
-//  * the wavefront condition is derived from the packed-column footprint of a hop ([cq, r1]):
-//    sweep s may run its hop once sweep s-1 has completed every hop that starts at or before
-//    r1, i.e. prog[s-1] >= r1 - b + 1.  That is a two-hop lag instead of the reference's
-//    four (prog >= c + 3b), which halves the pipeline fill.
+//  * the wavefront condition is derived from the footprints of the hops: hop h of sweep s
+//    (window rows [cq, r1 + b], reflector rows [r0, r1]) overlaps hop h+1 of sweep s-1 on a
+//    block and hop h+2 of sweep s-1 on one element only, A(r1 + b, r1) (the first entry of
+//    that hop's reduced column, which it sets to its beta and hop h later rewrites).  So hop h
+//    waits until sweep s-1 has completed hop h+1 (prog[s-1] >= r1 - b, the start of that hop)
+//    and has written the beta of hop h+2 (prog_ref[s-1] >= r1 - b + 1); hop h+2 writes that
+//    element right after its reflector is formed and publishes it, and leaves it alone in its
+//    update.  The reference waits for four hops (prog >= c + 3b).
 //  * per hop the b x 3b strip of the symmetric window that the reflector touches is gathered
 //    into shared memory once; each updated element (rank-2 H A H) goes straight back to the band
 //    from the thread that computes it, with no barrier between update and write-back.
@@ -34,13 +38,15 @@ template <int BW> struct ChaseSmem {
     double S[BW][3 * BW + 1]; // strip: S[k][ii] = A(lo + ii, r0 + k)
     double w[BW];             // reflector
     double p[3 * BW];         // p = 2 A w over the window rows
-    double red[2];            // beta, kappa
+    double beta;
+    double kap[BC_THREADS / 32]; // per-warp partial sums of kappa = w^T p
 };
 
 template <int BW>
 __global__ void __launch_bounds__(BC_THREADS)
     bc_chase_kernel(double *__restrict__ Bp, double *__restrict__ U, long long ldu, int n, int b,
                     int *prog, int *status) {
+    int *prog_ref = prog + n; // per sweep: cq of the last hop whose beta is in the band
     constexpr int NT = BC_THREADS;
     constexpr int NLEFT = (BW * BW + NT - 1) / NT;    // left-block elements per thread
     constexpr int NLOW = (2 * BW * BW + NT - 1) / NT; // lower-part elements per thread
@@ -67,7 +73,8 @@ __global__ void __launch_bounds__(BC_THREADS)
             const int W = hi - lo + 1;
             const int off = r0 - lo; // strip row of reflector row r0
 
-            // ---- wait for sweep s-1 to finish every hop that starts at or before r1
+            // ---- wait for sweep s-1: every hop that starts at or before r1 - b completed, and
+            // the beta of the hop that starts in (r1 - b, r1] written
             if (tid == 0) {
                 int ok = 1;
                 if (s > 0) {
@@ -77,7 +84,8 @@ __global__ void __launch_bounds__(BC_THREADS)
                     // the clock is read every 256 polls, or every poll under a short limit
                     const int every = limit < 1000000ull ? 0 : 255;
                     int spins = 0;
-                    while (ld_acquire(&prog[s - 1]) < need) {
+                    while (ld_acquire(&prog[s - 1]) < need - 1 ||
+                           ld_acquire(&prog_ref[s - 1]) < need) {
                         if ((++spins & every) == 0) {
                             if (global_ns() - t0 > limit ||
                                 ld_acquire(&status[DEV_STATUS_CODE]) != 0) {
@@ -127,54 +135,102 @@ __global__ void __launch_bounds__(BC_THREADS)
                 const int i = lo + ii, j = r0 + k;
                 if (ii < W && k < L && i >= j) sm.S[k][ii] = vw[q];
             }
-            __syncthreads();
-            // upper part of the diagonal block by symmetry; Householder of x = S[0:L][0]
-            for (int idx = tid; idx < BW * BW; idx += NT) {
-                const int a = idx % BW, k = idx / BW; // row r0+a, column r0+k
-                if (a < k && k < L) sm.S[k][off + a] = sm.S[a][off + k];
-            }
-            if (warp == 0) {
-                double ss = 0.0;
-                for (int k = lane; k < L; k += 32) {
-                    const double v = sm.S[k][0];
-                    ss += v * v;
+            // Householder of x = A(r0 : r1, cq).  b = 32: straight from the gathered registers
+            // (lane k of warp 0 holds x[k] in vl[0], the left-block element ii = 0, zero for
+            // k >= L), before the barrier; b = 64: from the strip after it.
+            if constexpr (BW == 32) {
+                if (warp == 0) {
+                    const double xk = vl[0];
+                    const double ss = warp_sum(xk * xk);
+                    const double x0 = __shfl_sync(0xffffffffu, xk, 0);
+                    double wk = 0.0;
+                    if (ss != 0.0) {
+                        const double beta = (x0 >= 0.0) ? -sqrt(ss) : sqrt(ss);
+                        const double v0 = x0 - beta;
+                        wk = (lane == 0 ? v0 : xk) * rsqrt(v0 * v0 + (ss - x0 * x0));
+                        if (lane == 0) sm.beta = beta;
+                    } else if (lane == 0) {
+                        sm.beta = 0.0;
+                    }
+                    sm.w[lane] = wk;
                 }
-                ss = warp_sum(ss);
-                const double x0 = sm.S[0][0];
-                if (ss == 0.0) {
-                    for (int k = lane; k < L; k += 32) sm.w[k] = 0.0;
-                    if (lane == 0) sm.red[0] = 0.0;
-                } else {
-                    const double sgn = (x0 >= 0.0) ? 1.0 : -1.0;
-                    const double beta = -sgn * sqrt(ss);
-                    const double v0 = x0 - beta;
-                    const double inv = 1.0 / sqrt(v0 * v0 + (ss - x0 * x0));
-                    for (int k = lane; k < L; k += 32) sm.w[k] = (k == 0 ? v0 : sm.S[k][0]) * inv;
-                    if (lane == 0) sm.red[0] = beta;
+                __syncthreads();
+            } else {
+                __syncthreads();
+                if (warp == 0) {
+                    double ss = 0.0;
+                    for (int k = lane; k < L; k += 32) ss = fma(sm.S[k][0], sm.S[k][0], ss);
+                    ss = warp_sum(ss);
+                    const double x0 = sm.S[0][0];
+                    if (ss == 0.0) {
+                        for (int k = lane; k < BW; k += 32) sm.w[k] = 0.0;
+                        if (lane == 0) sm.beta = 0.0;
+                    } else {
+                        const double beta = (x0 >= 0.0) ? -sqrt(ss) : sqrt(ss);
+                        const double v0 = x0 - beta;
+                        const double inv = rsqrt(v0 * v0 + (ss - x0 * x0));
+                        for (int k = lane; k < BW; k += 32)
+                            sm.w[k] = k < L ? (k == 0 ? v0 : sm.S[k][0]) * inv : 0.0;
+                        if (lane == 0) sm.beta = beta;
+                    }
                 }
+                __syncthreads();
             }
-            __syncthreads();
 
-            // ---- p = 2 A w over the window rows
-            for (int ii = tid; ii < W; ii += NT) {
-                // four chains: this dot product is on the hop's critical path
-                double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-                int k = 0;
-                for (; k + 3 < L; k += 4) {
-                    a0 = fma(sm.S[k][ii], sm.w[k], a0);
-                    a1 = fma(sm.S[k + 1][ii], sm.w[k + 1], a1);
-                    a2 = fma(sm.S[k + 2][ii], sm.w[k + 2], a2);
-                    a3 = fma(sm.S[k + 3][ii], sm.w[k + 3], a3);
+            // ---- p = 2 A w over the window rows (TPR threads per row, the upper half of the
+            // diagonal block read from its mirror), and per-warp partial sums of
+            // kappa = w^T p over the reflector rows (rows off .. off + L - 1)
+            {
+                constexpr int TPR = (NT >= 2 * 3 * BW) ? 2 : 1;
+                constexpr int KP = BW / TPR;                 // k range per thread
+                constexpr int PW = (3 * BW * TPR + 31) / 32; // warps that hold rows
+                static_assert(PW < NT / 32, "the last warp holds no row");
+                const int h = tid % TPR, ii = tid / TPR; // every lane of a row warp shuffles
+                const bool act = ii < W;
+                double kp = 0.0;
+                if (tid == NT - 1) {
+                    // this hop's beta, A(r0, cq), for the next sweep (see the wait above); the
+                    // release orders the store before the flag
+                    __stcg(&Bp[(r0 - cq) + (long long)cq * ldb], sm.beta);
+                    st_release(&prog_ref[s], cq);
                 }
-                for (; k < L; ++k) a0 = fma(sm.S[k][ii], sm.w[k], a0);
-                sm.p[ii] = 2.0 * ((a0 + a1) + (a2 + a3));
+                if (warp < PW) {
+                    const int a = ii - off; // row within the diagonal block when 0 <= a < L
+                    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+                    const int k0 = h * KP, k1 = act ? min(L, k0 + KP) : k0;
+                    int k = k0;
+                    if (a >= 0 && a < L) {
+                        // (an unconditional split of this loop at k = a made the compiler
+                        // schedule the update phase below 1300 cycles slower per hop)
+                        for (; k < k1; ++k) {
+                            const double v = k > a ? sm.S[a][off + k] : sm.S[k][ii];
+                            a0 = fma(v, sm.w[k], a0);
+                        }
+                    } else {
+                        for (; k + 3 < k1; k += 4) {
+                            a0 = fma(sm.S[k][ii], sm.w[k], a0);
+                            a1 = fma(sm.S[k + 1][ii], sm.w[k + 1], a1);
+                            a2 = fma(sm.S[k + 2][ii], sm.w[k + 2], a2);
+                            a3 = fma(sm.S[k + 3][ii], sm.w[k + 3], a3);
+                        }
+                        for (; k < k1; ++k) a0 = fma(sm.S[k][ii], sm.w[k], a0);
+                    }
+                    double pr = (a0 + a1) + (a2 + a3);
+                    if constexpr (TPR == 2) pr += __shfl_xor_sync(0xffffffffu, pr, 1);
+                    pr *= 2.0;
+                    if (act && h == 0) {
+                        sm.p[ii] = pr;
+                        if (a >= 0 && a < L) kp = fma(sm.w[a], pr, kp);
+                    }
+                }
+                if (warp < PW) kp = warp_sum(kp);
+                if (lane == 0) sm.kap[warp] = kp;
             }
             __syncthreads();
-            // kappa = w^T p over the reflector rows (every warp computes it)
-            double kl = 0.0;
-            for (int k = lane; k < L; k += 32) kl += sm.w[k] * sm.p[off + k];
-            const double kappa = warp_sum(kl);
-            const double beta = sm.red[0];
+            double kappa = 0.0;
+#pragma unroll
+            for (int q = 0; q < NT / 32; ++q) kappa += sm.kap[q];
+            const double beta = sm.beta;
 
             for (int k = tid; k < L; k += NT) U[(r0 + k) + (long long)s * ldu] = sm.w[k];
 
@@ -188,9 +244,10 @@ __global__ void __launch_bounds__(BC_THREADS)
                 const int idx = tid + q * NT;
                 const int k = idx % BW, ii = idx / BW;
                 if (ii >= off || k >= L) continue;
+                if (ii == 0 && k == 0) continue; // beta: written before the p phase
                 double v;
                 if (ii == 0) {
-                    v = (k == 0) ? beta : 0.0;
+                    v = 0.0;
                 } else { // kr = ii - off < 0: w_row = 0
                     v = sm.S[k][ii] - sm.p[ii] * sm.w[k];
                 }
@@ -212,13 +269,17 @@ __global__ void __launch_bounds__(BC_THREADS)
                 __stcg(&Bp[(i - j) + (long long)j * ldb], sm.S[k][ii] - (wr * yc + yr * wk));
             }
 
-            // ---- publish: the barrier orders every thread's stores before thread 0's release
-            // (release is cumulative over what thread 0 has observed through the barrier)
+            // ---- publish: the barrier orders every thread's stores before the release (which is
+            // cumulative over what the releasing thread has observed through the barrier).  The
+            // last thread releases, so that thread 0 goes on to the next hop's wait while the
+            // release's fence drains; the same thread publishes the end of the sweep below, so
+            // prog[s] only grows.
             __syncthreads();
-            if (tid == 0) st_release(&prog[s], cq);
+            if (tid == NT - 1) st_release(&prog[s], cq);
         }
-        if (tid == 0) {
+        if (tid == NT - 1) {
             __threadfence();
+            st_release(&prog_ref[s], INT_MAX);
             st_release(&prog[s], INT_MAX);
         }
         __syncthreads();
@@ -260,8 +321,8 @@ int bc_chase(Workspace *ws, double *B, double *d, double *e) {
     const int n = ws->n, b = ws->b;
     CUEV_TRY(cudaMemsetAsync(ws->U, 0, sizeof(double) * (size_t)n * n, ws->stream));
     if (n > 2) {
-        // prog = -1: no hop completed yet
-        CUEV_TRY(cudaMemsetAsync(ws->prog, 0xFF, sizeof(int) * (size_t)n, ws->stream));
+        // prog, prog_ref = -1: no hop completed, no beta written yet
+        CUEV_TRY(cudaMemsetAsync(ws->prog, 0xFF, 2 * sizeof(int) * (size_t)n, ws->stream));
         if (b == 32)
             CUEV_CHECK_STATUS(launch_chase<32>(ws, B));
         else if (b == 64)

@@ -32,7 +32,7 @@ struct Workspace {
     double *Y = nullptr, *Z = nullptr, *Wp = nullptr, *Tp = nullptr, *Tblk = nullptr;
     double *tau = nullptr, *Dwk = nullptr, *Cwk = nullptr, *Gblk = nullptr;
     double *B = nullptr, *U = nullptr, *d = nullptr, *e = nullptr;
-    int *prog = nullptr;
+    int *prog = nullptr; // 2n words: bulge-chase progress per sweep (hops done, betas written)
     unsigned *bar = nullptr; // grid-barrier words for cooperative kernels
     int *status = nullptr;   // device status words (DEV_STATUS_WORDS ints)
     double *dc_flops = nullptr; // flops of the D&C merge GEMMs of the last tridi_dc (after deflation)

@@ -59,7 +59,7 @@ int workspace_create(int n, int b, int k, cudaStream_t stream, Workspace **out) 
         {(void **)&ws->B, 2 * (size_t)b * N * s},
         {(void **)&ws->d, N * s},
         {(void **)&ws->e, N * s},
-        {(void **)&ws->prog, N * sizeof(int)},
+        {(void **)&ws->prog, 2 * N * sizeof(int)}, // chase: hops done, betas written
         {(void **)&ws->bar, 64},
         {(void **)&ws->status, DEV_STATUS_WORDS * sizeof(int)},
         {(void **)&ws->dc_flops, sizeof(double)},
