@@ -511,7 +511,7 @@ def run_cuev(args, rank, world, local_rank):
         "dbbr": {"tflops": round((4.0 / 3.0) * n ** 3 / (med["dbbr_ms"] * 1e-3) / 1e12, 3)},
         "bulge_chase": {"l2_gbs_model": round(48.0 * n * n * 32 / (med["bc_ms"] * 1e-3) / 1e9, 1),
                         "note": "48 n^2 b bytes (the 2b x 3b window read and written per hop), "
-                                "b = 32; latency bound (about 2n + n/b dependent hops)"},
+                                "b = 32; latency bound (per sweep two hops and a reflector on the critical path)"},
         "divide_and_conquer": {"tflops": round(dc_flops / (med["dc_ms"] * 1e-3) / 1e12, 3),
                                "merge_gflop": round(dc_flops / 1e9, 1),
                                "note": "merge GEMM flops counted on the device after deflation "
