@@ -2,7 +2,7 @@
 //
 // tcgen05 has no f64 kind, so FP64 contractions run on the DMMA path
 // (`mma.sync.aligned.m16n8k8.row.col.f64`), fed by a multi-stage cp.async shared-memory
-// pipeline.  One kernel template covers every contraction the solver needs:
+// pipeline synchronised on mbarriers.  One kernel template covers every contraction the solver needs:
 //   - plain GEMM with op(A), op(B) in {N, T}                       (reference cublas::gemm)
 //   - SYMM with A symmetric, lower triangle read                  (reference cublas::symm LOWER)
 //   - SYR2K as one GEMM over a two-segment K: [A1 | A2] [B1 | B2]^T, lower triangle written
@@ -41,6 +41,11 @@ int gemm_launch(const GemmArgs &a, int ta, int tb, cudaStream_t stream);
 // ta/tb, no split-K).  max_m/max_n bound every problem's m/n (they size the grid).
 int gemm_batched_launch(const GemmArgs *dev_args, int count, int max_m, int max_n, int ta, int tb,
                         cudaStream_t stream);
+
+// Records CUEV_ERR_TIMEOUT (detail -100) in `status` (stream ordered) if a stage wait of any GEMM
+// has given up since the library was loaded (sticky; the waits only depend on the CTA's own
+// copies, so this means a device fault).
+int gemm_fold_fault(int *status, cudaStream_t stream);
 
 // Split-K workspace needed by gemm_launch for a problem (0 when no split is used).
 size_t gemm_splitk_workspace(int m, int n, int k_total, int ta, int tb, int c_lower);

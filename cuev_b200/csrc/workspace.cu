@@ -144,6 +144,7 @@ void workspace_destroy(Workspace *ws) {
 
 int workspace_check_status(Workspace *ws, const char *stage) {
     int h[DEV_STATUS_WORDS] = {0};
+    CUEV_CHECK_STATUS(gemm_fold_fault(ws->status, ws->stream));
     CUEV_TRY(cudaMemcpyAsync(h, ws->status, sizeof(h), cudaMemcpyDeviceToHost, ws->stream));
     CUEV_TRY(cudaStreamSynchronize(ws->stream));
     if (h[DEV_STATUS_CODE] != 0) {
