@@ -26,7 +26,7 @@ struct TileCfg {
     static_assert((BN / 2) * BK % NT == 0 && (BN / 2) * BK / NT >= 1, "B tile / threads");
 };
 
-using CfgBig = TileCfg<128, 128, 4, 4, 3, 8, 32>; // 16 warps (two per SMSP left the DMMA pipe idle), BK 32
+using CfgBig = TileCfg<128, 128, 4, 4, 3, 16, 32>; // 16 warps (two per SMSP left the DMMA pipe idle), BK 32, k16 DMMA
 // batched (D&C merge) problems read with 8-byte copies, where 32-deep stages are slower
 using CfgBigBatched = TileCfg<128, 128, 4, 4, 4, 8>;
 using CfgSkinny = TileCfg<128, 64, 4, 2, 4>;
