@@ -27,8 +27,10 @@ struct TileCfg {
 };
 
 using CfgBig = TileCfg<128, 128, 4, 4, 3, 16, 32>; // 16 warps (two per SMSP left the DMMA pipe idle), BK 32, k16 DMMA
-// batched (D&C merge) problems read with 8-byte copies, where 32-deep stages are slower
-using CfgBigBatched = TileCfg<128, 128, 4, 4, 4, 8>;
+// batched (D&C merge) problems read with 8-byte copies; on the mbarrier pipeline 32-deep stages
+// and k16 beat 16-deep ones (D&C stage 213 -> 194 ms at n = 16384; they were slower with a CTA
+// barrier per stage)
+using CfgBigBatched = TileCfg<128, 128, 4, 4, 3, 16, 32>;
 using CfgSkinny = TileCfg<128, 64, 4, 2, 4>;
 using CfgSmall = TileCfg<64, 64, 2, 2, 4>;
 using CfgN32 = TileCfg<128, 32, 8, 1, 4>; // N <= 32 (band width 32 panels): 16 x 32 warp tiles
