@@ -20,6 +20,8 @@ Reported (one JSON line on rank 0):
   mixed_refine  the precision form (cuev_dsyevd_mixed) on the same matrix: time, speed-up over
              the FP64 form, refinement steps and accuracy (outside the headline's timed region)
   fwd_bwd    forward solve + adjoint (cuev_dsyev_adjoint) at n and at 4096
+  fp32_entry  the FP32 entry (cuev_ssyevd, BC-back in FP32) on the same matrix rounded to FP32:
+             time, speed-up over the FP64 form, stage times and accuracy
 The reference arm (--impl reference) runs the reference built from its own sources
 (oracle/_ref/ref_driver) on the same matrix, steps and warm-up where that build and a GPU exist,
 else the oracle port on a bounded CPU sample.
@@ -451,6 +453,51 @@ def run_cuev(args, rank, world, local_rank):
                  "accuracy": {"resid_n_norm2": m_resid, "orth_fro": m_orth,
                               "max_dlambda_vs_fp64_rel": m_dl}}
 
+    # ---- FP32 entry (cuev_ssyevd) on the same matrix rounded to FP32
+    fp32 = None
+    if not args.no_fp32:
+        A32 = A0.to(torch.float32)
+        Aw = torch.empty_like(A32)
+        w32 = torch.empty(n, dtype=torch.float32, device=dev)
+        V32 = torch.empty_like(A32)
+        ftimer = cv.Timer()
+        fts, fparts = [], []
+        for r_ in range(1 + max(1, min(args.steps, 3))):  # the first run is a warm-up
+            Aw.copy_(A32)
+            f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            f0.record(stream)
+            st = lib.cuev_ssyevd(Aw.data_ptr(), n, w32.data_ptr(), V32.data_ptr(), sp,
+                                 C.byref(ftimer))
+            f1.record(stream)
+            torch.cuda.synchronize()
+            if st != 0:
+                raise RuntimeError(f"cuev_ssyevd failed: {st} {lib.cuev_last_error().decode()}")
+            if r_ >= 1:
+                fts.append(f0.elapsed_time(f1))
+                fparts.append({k2: getattr(ftimer, k2) for k2 in ("dbbr_ms", "bc_ms", "dc_ms",
+                                                                   "bt_ms")})
+        fms = max_over_ranks(statistics.median(fts), dist, dev)
+        with torch.no_grad():
+            A64 = A32.to(torch.float64)
+            Vl = V32.t().to(torch.float64)
+            wl = w32.to(torch.float64)
+            R = A64 @ Vl - Vl * wl[None, :]
+            f_resid = float(torch.linalg.norm(R) / torch.linalg.norm(A64))
+            del R
+            O_ = Vl.t() @ Vl
+            O_.diagonal().sub_(1.0)
+            f_orth = float(torch.linalg.norm(O_) / n ** 0.5)
+            del O_, Vl, A64
+            torch.cuda.empty_cache()
+        fp32 = {"form": "cuev_ssyevd: FP64 band reduction, chase and D&C; BC-back in FP32; "
+                        "SBR-back on FP32-level int8 tensor-core products",
+                "ms_per_step": round(fms, 3),
+                "speedup_vs_fp64": round(ms_per / fms, 3),
+                "stage_ms": {k2: round(statistics.median(p_[k2] for p_ in fparts), 2)
+                             for k2 in ("dbbr_ms", "bc_ms", "dc_ms", "bt_ms")},
+                "accuracy": {"resid_fro_rel": f_resid, "orth_fro_per_sqrt_n": f_orth}}
+        del A32, Aw, V32, w32
+
     # ---- differentiation form: forward solve + adjoint (backward), at n and at 4096
     fwd_bwd = None
     if not args.no_adjoint:
@@ -565,6 +612,7 @@ def run_cuev(args, rank, world, local_rank):
             "stage_roofline": stage_rf,
             "mixed_refine": mixed,
             "fwd_bwd": fwd_bwd,
+            "fp32_entry": fp32,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "clocks": clk,
@@ -589,6 +637,7 @@ def main(argv=None):
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--no-fp32", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--mixed-iters", type=int, default=1)
     args = ap.parse_args(argv)

@@ -28,10 +28,13 @@
 namespace cuev {
 namespace {
 
-__device__ __forceinline__ void cp_async8(double *smem, const double *gmem, bool pred) {
+// One-element asynchronous copy (4 or 8 bytes); pred false: zero fill, nothing read.
+template <typename T>
+__device__ __forceinline__ void cp_async_el(T *smem, const T *gmem, bool pred) {
+    constexpr int B = sizeof(T);
     const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gmem),
-                 "r"(pred ? 8 : 0)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(sa), "l"(gmem), "n"(B),
+                 "r"(pred ? B : 0)
                  : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
@@ -43,6 +46,15 @@ template <int N> __device__ __forceinline__ void cp_async_wait() {
 // asm loads made it hoist them and spill).
 __device__ __forceinline__ double2 lds2(const double *p) {
     return *reinterpret_cast<const double2 *>(p);
+}
+// 16-byte shared load into r[0 .. VN) (VN = 2 doubles or 4 floats)
+__device__ __forceinline__ void lds16(const double *p, double *r) {
+    const double2 v = *reinterpret_cast<const double2 *>(p);
+    r[0] = v.x, r[1] = v.y;
+}
+__device__ __forceinline__ void lds16(const float *p, float *r) {
+    const float4 v = *reinterpret_cast<const float4 *>(p);
+    r[0] = v.x, r[1] = v.y, r[2] = v.z, r[3] = v.w;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -74,10 +86,10 @@ __device__ __forceinline__ double2 lds2(const double *p) {
 // final for tile t once its hop h is done; and a reflector (s', h') of tile t - 1 commutes with
 // every (s, h'') of tile t with h'' >= h' + 1 (their rows are disjoint), so running tile t - 1 one
 // hop block behind tile t applies the reflectors in an order equivalent to the reverse order.
-template <int TS, int P, int PB> struct PipeSmem {
-    double w[P][2][TS][PB];        // reflectors of each warp's current and next hop block
-    double ring[P - 1][2][PB][32]; // warp p -> warp p+1, two chunks of PB rows x 32 columns
-    double xin[2][PB][32];         // warp 0: incoming rows (from X or, first tile, from M)
+template <typename T, int TS, int P, int PB> struct PipeSmem {
+    T w[P][2][TS][PB];        // reflectors of each warp's current and next hop block
+    T ring[P - 1][2][PB][32]; // warp p -> warp p+1, two chunks of PB rows x 32 columns
+    T xin[2][PB][32];         // warp 0: incoming rows (from X or, first tile, from M)
     int prod[P], cons[P];          // ring p: chunks written / chunks fully read (monotonic)
     int gprog;                     // chunks the last warp has written to X (monotonic)
     int abort_flag;                // set by a warp that gave up waiting
@@ -122,23 +134,24 @@ __device__ __forceinline__ bool pipe_wait(const int *flag, int target, int *abor
     }
 }
 
-template <int TS, int P, int PB>
+template <typename T, int TS, int P, int PB>
 __global__ void __launch_bounds__(32 * P, 1)
-    bc_back_pipe_kernel(const double *__restrict__ U, long long ldu, double *__restrict__ M,
-                        long long ldm, double *__restrict__ X, int n, int ncols,
+    bc_back_pipe_kernel(const T *__restrict__ U, long long ldu, T *__restrict__ M,
+                        long long ldm, T *__restrict__ X, int n, int ncols,
                         int *__restrict__ status) {
-    static_assert(PB == 32 || PB == 64, "band width 32 or 64");
-    constexpr int R = TS + PB; // register window rows
+    static_assert(PB == 32 || (PB == 64 && sizeof(T) == 8), "band width 32 (or 64, FP64)");
+    constexpr int R = TS + PB;          // register window rows
+    constexpr int VN = 16 / sizeof(T);  // elements per 16-byte copy or shared load
     extern __shared__ __align__(16) unsigned char pipe_smem_raw[];
-    PipeSmem<TS, P, PB> &S = *reinterpret_cast<PipeSmem<TS, P, PB> *>(pipe_smem_raw);
+    PipeSmem<T, TS, P, PB> &S = *reinterpret_cast<PipeSmem<T, TS, P, PB> *>(pipe_smem_raw);
     const int lane = threadIdx.x & 31, p = threadIdx.x >> 5;
     const int col0 = blockIdx.x * 32;
     const int mycol = min(col0 + lane, ncols - 1); // clamped: lanes past ncols never store to M
     const bool active = col0 + lane < ncols;
-    const double *Mc = M + (long long)mycol * ldm;
-    double *Xg = X + (size_t)blockIdx.x * n * 32; // row r of this CTA's columns: Xg[32 r + lane]
+    const T *Mc = M + (long long)mycol * ldm;
+    T *Xg = X + (size_t)blockIdx.x * n * 32; // row r of this CTA's columns: Xg[32 r + lane]
     const int nsweeps = n - 2;
-    const int T = (nsweeps + TS - 1) / TS;
+    const int ntiles = (nsweeps + TS - 1) / TS;
     if (threadIdx.x < P) S.prod[threadIdx.x] = 0, S.cons[threadIdx.x] = 0;
     if (threadIdx.x == 0) S.gprog = 0, S.abort_flag = 0;
     __syncthreads(); // the only CTA-wide barrier: warps leave at different times
@@ -151,16 +164,16 @@ __global__ void __launch_bounds__(32 * P, 1)
             for (int t = 0; t < PB / 32; ++t) {
                 const int s = s0 + j, row = rbase + j + lane + 32 * t;
                 const bool ok = (s < nsweeps) && (row < n);
-                cp_async8(&S.w[p][buf][j][lane + 32 * t], ok ? U + row + (long long)s * ldu : U,
-                          ok);
+                cp_async_el(&S.w[p][buf][j][lane + 32 * t], ok ? U + row + (long long)s * ldu : U,
+                            ok);
             }
         }
     };
     // warp 0's incoming chunk: PB rows from X (coalesced 16-byte copies) ...
     auto stage_x = [&](int buf, int row0) {
 #pragma unroll
-        for (int q = 0; q < PB / 2; ++q) {
-            const int e = q * 64 + lane * 2; // element pair (row e / 32, columns e % 32, +1)
+        for (int q = 0; q < PB / VN; ++q) {
+            const int e = (q * 32 + lane) * VN; // VN elements: row e / 32, columns e % 32 ..
             const int r = row0 + (e >> 5);
             const bool ok = r < n;
             cp_async16_cg(&S.xin[buf][e >> 5][e & 31], ok ? Xg + (size_t)r * 32 + (e & 31) : Xg,
@@ -173,27 +186,27 @@ __global__ void __launch_bounds__(32 * P, 1)
     auto stage_m = [&](int buf, int row0) {
         if (row0 + PB <= n) {
 #pragma unroll
-            for (int i = 0; i < PB; ++i) cp_async8(&S.xin[buf][i][lane], Mc + row0 + i, true);
+            for (int i = 0; i < PB; ++i) cp_async_el(&S.xin[buf][i][lane], Mc + row0 + i, true);
         } else {
 #pragma unroll
             for (int i = 0; i < PB; ++i) {
                 const int r = row0 + i;
                 const bool ok = r < n;
-                cp_async8(&S.xin[buf][i][lane], ok ? Mc + r : Mc, ok);
+                cp_async_el(&S.xin[buf][i][lane], ok ? Mc + r : Mc, ok);
             }
         }
     };
 
-    double m[R];
+    T m[R];
     int oseq = 0;  // chunks this warp has put into ring p (or X, for the last warp)
     int iseq = 0;  // chunks this warp has taken from ring p-1
     int xbase = 0; // warp 0: X sequence number of the current input tile's chunk 0
     bool ok = true;
-    for (int t = T - 1 - p; t >= 0 && ok; t -= P) {
+    for (int t = ntiles - 1 - p; t >= 0 && ok; t -= P) {
         const int s0 = t * TS;
         const int top = s0 + 1;
         const int hmax = (n - 1 - top) / PB;
-        const bool has_in = t + 1 <= T - 1; // rows [top + TS, n) come from tile t + 1
+        const bool has_in = t + 1 <= ntiles - 1; // rows [top + TS, n) come from tile t + 1
         const int top_in = top + TS;
         const int hmax_in = has_in ? (n - 1 - top_in) / PB : -1;
         const bool first = !has_in; // only warp 0 of the first round
@@ -214,8 +227,8 @@ __global__ void __launch_bounds__(32 * P, 1)
 #pragma unroll
         for (int i = 0; i < TS; ++i) {
             const int row = top + i;
-            const double v = Mc[min(row, n - 1)];
-            m[i] = row < n ? v : 0.0;
+            const T v = Mc[min(row, n - 1)];
+            m[i] = row < n ? v : T(0);
         }
         for (int h = 0; h <= hmax; ++h) {
             const int base = top + h * PB; // row of m[0]
@@ -244,7 +257,7 @@ __global__ void __launch_bounds__(32 * P, 1)
                     for (int i = 0; i < PB; ++i) m[TS + i] = S.xin[h & 1][i][lane];
                 } else {
 #pragma unroll
-                    for (int i = 0; i < PB; ++i) m[TS + i] = 0.0;
+                    for (int i = 0; i < PB; ++i) m[TS + i] = T(0);
                 }
             } else if (h <= hmax_in) {
                 if (!pipe_wait(&S.prod[p - 1], iseq + 1, &S.abort_flag, status, -3)) {
@@ -259,27 +272,24 @@ __global__ void __launch_bounds__(32 * P, 1)
                 if (lane == 0) sts_release(&S.cons[p - 1], iseq);
             } else {
 #pragma unroll
-                for (int i = 0; i < PB; ++i) m[TS + i] = 0.0;
+                for (int i = 0; i < PB; ++i) m[TS + i] = T(0);
             }
 
             // apply the tile's reflectors of this hop, last sweep first
-            const double *W = &S.w[p][h & 1][0][0];
+            const T *W = &S.w[p][h & 1][0][0];
             if constexpr (PB == 32) {
 #pragma unroll
                 for (int j = TS - 1; j >= 0; --j) {
-                    double wr[PB];
+                    T wr[PB];
 #pragma unroll
-                    for (int i = 0; i < PB; i += 2) {
-                        const double2 v = lds2(W + j * PB + i);
-                        wr[i] = v.x, wr[i + 1] = v.y;
-                    }
-                    double acc[8];
+                    for (int i = 0; i < PB; i += VN) lds16(W + j * PB + i, &wr[i]);
+                    T acc[8];
 #pragma unroll
                     for (int i = 0; i < 8; ++i) acc[i] = wr[i] * m[j + i];
 #pragma unroll
                     for (int i = 8; i < PB; ++i) acc[i & 7] = fma(wr[i], m[j + i], acc[i & 7]);
-                    const double f = -2.0 * (((acc[0] + acc[1]) + (acc[2] + acc[3])) +
-                                             ((acc[4] + acc[5]) + (acc[6] + acc[7])));
+                    const T f = T(-2) * (((acc[0] + acc[1]) + (acc[2] + acc[3])) +
+                                         ((acc[4] + acc[5]) + (acc[6] + acc[7])));
 #pragma unroll
                     for (int i = 0; i < PB; ++i) m[j + i] = fma(f, wr[i], m[j + i]);
                 }
@@ -313,7 +323,7 @@ __global__ void __launch_bounds__(32 * P, 1)
             // rows [base, base + PB) are final for this tile
             if (to_m) {
                 if (active) {
-                    double *Mw = M + (long long)mycol * ldm + base;
+                    T *Mw = M + (long long)mycol * ldm + base;
                     if (base + PB <= n) {
 #pragma unroll
                         for (int i = 0; i < PB; ++i) Mw[i] = m[i];
@@ -324,7 +334,7 @@ __global__ void __launch_bounds__(32 * P, 1)
                     }
                 }
             } else if (to_x) {
-                double *Xr = Xg + (size_t)base * 32 + lane;
+                T *Xr = Xg + (size_t)base * 32 + lane;
                 if (base + PB <= n) {
 #pragma unroll
                     for (int i = 0; i < PB; ++i) __stcg(Xr + 32 * i, m[i]);
@@ -365,17 +375,30 @@ __global__ void __launch_bounds__(32 * P, 1)
 // Columns [c0, c0 + ncols) of M (c0 a multiple of 32): CTA g owns columns c0 + 32 g .. + 31 and
 // its hand-off rows in dc_S at the offset of its 32-column group, so launches over disjoint
 // column ranges are independent and together do what one launch over all columns does.
-template <int TS, int P, int PB>
-int launch_bc_back_pipe(Workspace *ws, cudaStream_t st, double *M, long long ldm, int c0,
+// dst (rows x cols, ld ldd) = src (ld lds), FP64 <-> FP32.
+template <typename S, typename D>
+__global__ void convert_cols_kernel(const S *__restrict__ src, long long lds, D *__restrict__ dst,
+                                    long long ldd, int rows, int cols) {
+    const long long total = (long long)rows * cols;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const long long c = idx / rows, r = idx - c * rows;
+        dst[r + c * ldd] = (D)src[r + c * lds];
+    }
+}
+
+template <typename T, int TS, int P, int PB>
+int launch_bc_back_pipe(Workspace *ws, cudaStream_t st, const T *U, T *M, long long ldm, int c0,
                         int ncols) {
     const int n = ws->n;
     if (ncols <= 0) return CUEV_OK;
-    const size_t smem = sizeof(PipeSmem<TS, P, PB>);
-    auto kern = bc_back_pipe_kernel<TS, P, PB>;
+    const size_t smem = sizeof(PipeSmem<T, TS, P, PB>);
+    auto kern = bc_back_pipe_kernel<T, TS, P, PB>;
     CUEV_CHECK_STATUS(ensure_dyn_smem((const void *)kern, smem));
     const int grid = div_up(ncols, 32);
-    double *Xc = ws->dc_S + (size_t)(c0 / 32) * n * 32;
-    kern<<<grid, 32 * P, smem, st>>>(ws->U, ws->n, M + (long long)c0 * ldm, ldm, Xc, n, ncols,
+    // hand-off rows in dc_S (n x n doubles: room for either element type)
+    T *Xc = reinterpret_cast<T *>(ws->dc_S) + (size_t)(c0 / 32) * n * 32;
+    kern<<<grid, 32 * P, smem, st>>>(U, ws->n, M + (long long)c0 * ldm, ldm, Xc, n, ncols,
                                      ws->status);
     note_launch();
     CUEV_TRY(cudaGetLastError());
@@ -399,9 +422,38 @@ int bt_gemm(Workspace *ws, int ta, int tb, int m, int n, int k, double alpha, co
 // streamed from shared memory), which is what fits 227 KB of shared memory with two-chunk rings.
 int launch_bc_back_cols(Workspace *ws, cudaStream_t st, double *M, long long ldm, int c0,
                         int ncols) {
-    if (ws->b == 32) return launch_bc_back_pipe<16, 8, 32>(ws, st, M, ldm, c0, ncols);
-    if (ws->b == 64) return launch_bc_back_pipe<8, 4, 64>(ws, st, M, ldm, c0, ncols);
+    if (ncols <= 0) return CUEV_OK;
+    if (ws->b == 32 && ws->fp32) {
+        // FP32 entry: the column range in FP32 (Mf, ld n) against U's float copy (made by
+        // bc_back_prepare), 16 warps per CTA (the float window leaves the registers for them)
+        const int n = ws->n;
+        const int blocks = std::min(4 * num_sms(), div_up((long long)n * ncols, 256));
+        convert_cols_kernel<<<blocks, 256, 0, st>>>(M + (long long)c0 * ldm, ldm,
+                                                    ws->Mf + (long long)c0 * n, n, n, ncols);
+        note_launch();
+        CUEV_TRY(cudaGetLastError());
+        CUEV_CHECK_STATUS(
+            (launch_bc_back_pipe<float, 16, 16, 32>(ws, st, ws->Uf, ws->Mf, n, c0, ncols)));
+        convert_cols_kernel<<<blocks, 256, 0, st>>>(ws->Mf + (long long)c0 * n, n,
+                                                    M + (long long)c0 * ldm, ldm, n, ncols);
+        note_launch();
+        CUEV_TRY(cudaGetLastError());
+        return CUEV_OK;
+    }
+    if (ws->b == 32) return launch_bc_back_pipe<double, 16, 8, 32>(ws, st, ws->U, M, ldm, c0, ncols);
+    if (ws->b == 64) return launch_bc_back_pipe<double, 8, 4, 64>(ws, st, ws->U, M, ldm, c0, ncols);
     return CUEV_ERR_INVALID;
+}
+
+// The FP32 entry's BC-back reads a float copy of the reflectors.
+int bc_back_prepare(Workspace *ws, cudaStream_t st) {
+    if (!(ws->fp32 && ws->b == 32) || ws->n <= 2) return CUEV_OK;
+    const int n = ws->n;
+    const int blocks = std::min(4 * num_sms(), div_up((long long)n * n, 256));
+    convert_cols_kernel<<<blocks, 256, 0, st>>>(ws->U, n, ws->Uf, n, n, n);
+    note_launch();
+    CUEV_TRY(cudaGetLastError());
+    return CUEV_OK;
 }
 
 // M <- Q_s M on ncols columns of M, with X (w x ncols) and X2 (w x ncols) as scratch.
@@ -432,6 +484,7 @@ int sbr_back_cols(Workspace *ws, double *M, long long ldm, int ncols, double *X,
 
 int bc_back(Workspace *ws, double *M, long long ldm) {
     if (ws->n <= 2) return CUEV_OK;
+    CUEV_CHECK_STATUS(bc_back_prepare(ws, ws->stream));
     return launch_bc_back_cols(ws, ws->stream, M, ldm, 0, ws->n);
 }
 
@@ -449,10 +502,11 @@ int sbr_back(Workspace *ws, double *M, long long ldm) {
 // the late BC-back's hand-off rows live in dc_S.
 int back_transform(Workspace *ws, double *M, long long ldm, cudaEvent_t bc_end) {
     const int n = ws->n;
+    if (n > 2) CUEV_CHECK_STATUS(bc_back_prepare(ws, ws->stream));
     const int groups = div_up(std::max(n, 1), 32);
     const int full = groups / num_sms() * num_sms(); // groups in whole waves
     if (n <= 2 || full == 0 || full == groups || !ws->side) {
-        CUEV_CHECK_STATUS(bc_back(ws, M, ldm));
+        if (n > 2) CUEV_CHECK_STATUS(launch_bc_back_cols(ws, ws->stream, M, ldm, 0, n));
         if (bc_end) CUEV_TRY(cudaEventRecord(bc_end, ws->stream));
         return sbr_back(ws, M, ldm);
     }

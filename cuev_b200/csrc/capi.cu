@@ -109,7 +109,7 @@ struct EventSet {
 struct MixedFlag {
     Workspace *ws;
     ~MixedFlag() {
-        if (ws) ws->mixed = 0;
+        if (ws) ws->mixed = 0, ws->fp32 = 0;
     }
 };
 
@@ -121,6 +121,7 @@ struct MixedReq {
     int max_iters;
     double tol;
     cuev_mixed_info *info;
+    bool fp32_bc_back = false; // FP32 entry: BC-back in FP32
 };
 
 int solve_d(double *A, int n, double *eval, double *evec, cudaStream_t stream, cuev_timer *timer,
@@ -165,6 +166,10 @@ int solve_d(double *A, int n, double *eval, double *evec, cudaStream_t stream, c
         // the refinement measures against the original A: keep it as FP64-level slices
         if (mixed->refine) CUEV_CHECK_STATUS(i8_slice(A, n, I8_SRC_SYML, ws->a_sl, stream));
         ws->mixed = 1;
+        if (mixed->fp32_bc_back && ws->b == 32) {
+            CUEV_CHECK_STATUS(workspace_enable_fp32(ws));
+            ws->fp32 = 1;
+        }
         mflag.ws = ws;
     }
     CUEV_CHECK_STATUS(rec(0));
@@ -271,9 +276,10 @@ extern "C" int cuev_ssyevd(float *A, int n, float *eval, float *evec, void *stre
     double *A64 = buf, *V64 = buf + nn, *w64 = buf + 2 * nn;
     const int blocks = 4 * num_sms();
     widen_kernel<<<blocks, 256, 0, st>>>(A, A64, nn); note_launch();
-    // FP32 results need FP32 accuracy only: the back-transform's large products run on the int8
-    // tensor cores at FP32 level (the precision form's first solve, without refinement)
-    MixedReq first_only{false, 0, 0.0, nullptr};
+    // FP32 results need FP32 accuracy only: BC-back runs in FP32 (b = 32) and the back-transform's
+    // large products on the int8 tensor cores at FP32 level (the precision form's first solve,
+    // without refinement)
+    MixedReq first_only{false, 0, 0.0, nullptr, true};
     int s = solve_d(A64, n, w64, evec ? V64 : nullptr, st, timer, nullptr,
                     evec ? &first_only : nullptr);
     if (s == CUEV_OK) {

@@ -61,6 +61,11 @@ struct Workspace {
     I8Operand a_sl;
     void *i8_scratch = nullptr;
     size_t i8_scratch_bytes = 0;
+    // FP32 entry: while `fp32` is set (b = 32), BC-back runs in FP32 on float copies of U and of
+    // the eigenvector columns (f32_pool: Uf and Mf, n x n floats each)
+    int fp32 = 0;
+    void *f32_pool = nullptr;
+    float *Uf = nullptr, *Mf = nullptr;
 
     void *pool = nullptr;
     size_t pool_bytes = 0;
@@ -70,6 +75,8 @@ struct Workspace {
 int workspace_create(int n, int b, int k, cudaStream_t stream, Workspace **out);
 // Allocate the precision form's buffers (GEMM slices; with_a_slices: also A's slices).
 int workspace_enable_mixed(Workspace *ws, bool with_a_slices);
+// Allocate the FP32 entry's float copies of U and of the eigenvectors.
+int workspace_enable_fp32(Workspace *ws);
 void workspace_destroy(Workspace *ws);
 // Check the device status word (synchronises the stream); returns its cuev_status.
 int workspace_check_status(Workspace *ws, const char *stage);

@@ -132,9 +132,27 @@ int workspace_enable_mixed(Workspace *ws, bool with_a_slices) {
     return CUEV_OK;
 }
 
+int workspace_enable_fp32(Workspace *ws) {
+    if (ws->f32_pool) return CUEV_OK;
+    const size_t nn = (size_t)std::max(ws->n, 1) * std::max(ws->n, 1);
+    const size_t total = 2 * align256(nn * sizeof(float));
+    if (cudaMalloc(&ws->f32_pool, total) != cudaSuccess) {
+        cudaGetLastError();
+        ws->f32_pool = nullptr;
+        char msg[160];
+        snprintf(msg, sizeof(msg), "FP32 entry: allocation of %.2f GB failed", total / 1e9);
+        set_last_message(msg);
+        return CUEV_ERR_ALLOC;
+    }
+    ws->Uf = (float *)ws->f32_pool;
+    ws->Mf = (float *)((char *)ws->f32_pool + align256(nn * sizeof(float)));
+    return CUEV_OK;
+}
+
 void workspace_destroy(Workspace *ws) {
     if (!ws) return;
     if (ws->mx_pool) cudaFree(ws->mx_pool);
+    if (ws->f32_pool) cudaFree(ws->f32_pool);
     if (ws->side) cudaStreamSynchronize(ws->side), cudaStreamDestroy(ws->side);
     if (ws->ev_a) cudaEventDestroy(ws->ev_a);
     if (ws->ev_b) cudaEventDestroy(ws->ev_b);

@@ -73,10 +73,12 @@ int cuev_dsyevd_cfg(double *A, int n, double *eval, double *evec, void *stream, 
                     const cuev_config *cfg);
 
 /* FP32 interface.  Replaces cuev::symm_eig_solve<float> (reference src/cuda/solver.cu:78).
- * The float input is widened and solved by the FP64 band reduction, bulge chase, D&C and
- * BC-back, with the SBR-back products (the back-transform's GEMMs) on the int8 tensor cores at
- * FP32-level accuracy (the precision form's first solve, cuev_dsyevd_mixed without refinement);
- * the results are rounded back to FP32. */
+ * The float input is widened and solved by the FP64 band reduction, bulge chase and D&C; BC-back
+ * runs in FP32 (b = 32; on float copies of the reflectors and eigenvectors, n^2 floats each, kept
+ * with the cached workspace) and the SBR-back products (the back-transform's GEMMs) on the int8
+ * tensor cores at FP32-level accuracy (5 slices); the results are rounded back to FP32.
+ * Accuracy is FP32-level (residual and orthogonality per sqrt(n) about 2e-6 at n = 3072, 4e-6 at
+ * n = 16384). */
 int cuev_ssyevd(float *A, int n, float *eval, float *evec, void *stream, cuev_timer *timer);
 
 /* Batched eigensolver for many small matrices (no reference counterpart: the reference solves one
