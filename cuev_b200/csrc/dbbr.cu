@@ -18,6 +18,7 @@
 #include "solver.cuh"
 
 #include <algorithm>
+#include <mutex>
 #include <cooperative_groups.h>
 
 namespace cuev {
@@ -394,9 +395,23 @@ __global__ void pack_kernel(const double *__restrict__ A, long long lda, double 
 }
 
 // Largest cluster the cluster kernel can run with (16 needs the non-portable opt-in; 0 = none),
-// probed once per instantiation with the occupancy API at the full shared-memory size.
+// probed once per instantiation and device with the occupancy API at the full shared-memory size
+// (the function attributes it sets apply to the current device only).
 template <int BW> int panel_qr_cluster_max() {
-    static int cached = -1;
+    static int cache[64];
+    static bool init = false;
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lk(mu);
+    if (!init) {
+        for (int &c : cache) c = -1;
+        init = true;
+    }
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+        cudaGetLastError();
+        return 0;
+    }
+    int &cached = cache[dev];
     if (cached >= 0) return cached;
     cached = 0;
     auto kern = panel_qr_cluster_kernel<BW>;
