@@ -417,8 +417,9 @@ int bt_gemm(Workspace *ws, int ta, int tb, int m, int n, int k, double alpha, co
     return ws_gemm(ws, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
 }
 
-// BC-back over columns [c0, c0 + ncols): b = 32 runs 8 warps on 16-sweep tiles (79-row register
-// window, 252 registers); b = 64 runs 4 warps on 16-sweep tiles (80-row window, the reflector
+// BC-back over columns [c0, c0 + ncols): b = 32 runs 8 warps on 14-sweep tiles (46-row register
+// window; at n = 16384 tiles of 12, 13, 14, 15 and 16 sweeps took 587, 585, 574, 599 and 619 ms,
+// 8 sweeps or 10 warps spill); b = 64 runs 4 warps on 8-sweep tiles (72-row window, the reflector
 // streamed from shared memory), which is what fits 227 KB of shared memory with two-chunk rings.
 int launch_bc_back_cols(Workspace *ws, cudaStream_t st, double *M, long long ldm, int c0,
                         int ncols) {
@@ -440,7 +441,7 @@ int launch_bc_back_cols(Workspace *ws, cudaStream_t st, double *M, long long ldm
         CUEV_TRY(cudaGetLastError());
         return CUEV_OK;
     }
-    if (ws->b == 32) return launch_bc_back_pipe<double, 16, 8, 32>(ws, st, ws->U, M, ldm, c0, ncols);
+    if (ws->b == 32) return launch_bc_back_pipe<double, 14, 8, 32>(ws, st, ws->U, M, ldm, c0, ncols);
     if (ws->b == 64) return launch_bc_back_pipe<double, 8, 4, 64>(ws, st, ws->U, M, ldm, c0, ncols);
     return CUEV_ERR_INVALID;
 }

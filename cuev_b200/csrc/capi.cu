@@ -224,6 +224,17 @@ int solve_d(double *A, int n, double *eval, double *evec, cudaStream_t stream, c
     return CUEV_OK;
 }
 
+// FP32 entry: per-device widening buffer kept between calls (grown on demand; a stream-ordered
+// allocation and release of ~4 GB per call at n = 16384 cost several hundred ms); a call that finds
+// it in use on another thread takes a stream-ordered allocation instead.
+struct WidenBuf {
+    double *p = nullptr;
+    size_t bytes = 0;
+    bool busy = false;
+};
+std::mutex g_wb_mu;
+WidenBuf g_wb[64];
+
 __global__ void widen_kernel(const float *__restrict__ s, double *__restrict__ d, long long cnt) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < cnt;
          i += (long long)gridDim.x * blockDim.x)
@@ -267,8 +278,35 @@ extern "C" int cuev_ssyevd(float *A, int n, float *eval, float *evec, void *stre
     if (!A || !eval) return CUEV_ERR_INVALID; // evec == NULL: eigenvalues only
     cudaStream_t st = (cudaStream_t)stream;
     const long long nn = (long long)n * n;
+    const size_t need = sizeof(double) * (2 * nn + n);
+    int dev = 0;
+    CUEV_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return CUEV_ERR_INVALID;
     double *buf = nullptr;
-    if (cudaMallocAsync((void **)&buf, sizeof(double) * (2 * nn + n), st) != cudaSuccess) {
+    bool cached = false;
+    {
+        std::lock_guard<std::mutex> lk(g_wb_mu);
+        WidenBuf &wb = g_wb[dev];
+        if (!wb.busy) {
+            if (wb.bytes < need) {
+                if (wb.p) cudaFree(wb.p);
+                wb.p = nullptr;
+                wb.bytes = 0;
+                if (cudaMalloc((void **)&wb.p, need) == cudaSuccess) {
+                    wb.bytes = need;
+                } else {
+                    cudaGetLastError();
+                    wb.p = nullptr;
+                }
+            }
+            if (wb.p) {
+                wb.busy = true;
+                buf = wb.p;
+                cached = true;
+            }
+        }
+    }
+    if (!buf && cudaMallocAsync((void **)&buf, need, st) != cudaSuccess) {
         cudaGetLastError();
         set_last_message("FP32 entry: widening buffer allocation failed");
         return CUEV_ERR_ALLOC;
@@ -287,8 +325,12 @@ extern "C" int cuev_ssyevd(float *A, int n, float *eval, float *evec, void *stre
         narrow_kernel<<<1, 256, 0, st>>>(w64, eval, n); note_launch();
         narrow_kernel<<<blocks, 256, 0, st>>>(A64, A, nn); note_launch(); // A is clobbered like the reference's
     }
-    cudaFreeAsync(buf, st);
+    if (!cached) cudaFreeAsync(buf, st);
     if (cudaStreamSynchronize(st) != cudaSuccess && s == CUEV_OK) s = CUEV_ERR_CUDA;
+    if (cached) {
+        std::lock_guard<std::mutex> lk(g_wb_mu);
+        g_wb[dev].busy = false;
+    }
     return s;
 }
 
@@ -300,6 +342,20 @@ void batched_mid_release();
 
 extern "C" int cuev_release_workspace(void) {
     cuev::batched_mid_release();
+    {
+        std::lock_guard<std::mutex> lk(cuev::g_wb_mu);
+        int cur = 0;
+        if (cudaGetDevice(&cur) == cudaSuccess) {
+            for (int d = 0; d < 64; ++d)
+                if (cuev::g_wb[d].p && !cuev::g_wb[d].busy) {
+                    if (cudaSetDevice(d) == cudaSuccess) cudaFree(cuev::g_wb[d].p);
+                    cuev::g_wb[d].p = nullptr;
+                    cuev::g_wb[d].bytes = 0;
+                }
+            cudaSetDevice(cur);
+        }
+        cudaGetLastError();
+    }
     std::lock_guard<std::mutex> lk(g_cache_mu);
     for (auto &c : g_cache) {
         if (c.ws && !c.busy) {

@@ -158,7 +158,8 @@ int cuev_dsyevd_mixed(double *A, int n, double *eval, double *evec, void *stream
                       cuev_mixed_info *info);
 
 /* Release the cached device workspace (the solves keep one pool per (n, b, k) between calls, the
- * batched eigensolver one buffer per device for 64 < n <= 512). */
+ * batched eigensolver one buffer per device for 64 < n <= 512, the FP32 entry one widening buffer
+ * per device, (2 n^2 + n) doubles). */
 int cuev_release_workspace(void);
 
 /* Message for the last failing call on this host thread ("" if none). */
