@@ -547,7 +547,7 @@ def run_cuev(args, rank, world, local_rank):
         try:
             tj = json.loads(tfile.read_text())
             # DRAM bytes per launch grow as n^3: the round-to-round hand-off buffer (n x n) is
-            # written and read once per round of 8 sweep tiles (n / 128 rounds); M itself is
+            # written and read once per round of 8 sweep tiles (n / 112 rounds); M itself is
             # read and written once (n^2).  Scaled from one ncu capture at a smaller n.
             traffic = int(tj["dram_bytes"] * (n / tj["n"]) ** 3)
         except Exception:
