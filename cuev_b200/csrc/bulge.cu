@@ -303,7 +303,10 @@ template <int BW> int launch_chase(Workspace *ws, double *B) {
     CUEV_CHECK_STATUS(ensure_dyn_smem((const void *)kern, smem));
     int per_sm = 0;
     CUEV_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, BC_THREADS, smem));
-    const int cap = std::max(1, per_sm) * num_sms();
+    // at most two CTAs per SM: a hop's latency grows with the CTAs that share its SM, and two per
+    // SM still keep more sweeps in flight than the wavefront needs (n = 16384: 3 per SM 179.7 ms,
+    // 2 per SM 175.6, 1 per SM 176.1)
+    const int cap = std::min(2, std::max(1, per_sm)) * num_sms();
     int grid = std::max(1, std::min(nsweeps, cap));
     double *U = ws->U;
     long long ldu = n;
