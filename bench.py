@@ -9,8 +9,9 @@ workload is n = 16384, the size the reference's headline throughput is quoted on
 Reported (one JSON line on rank 0):
   value      whole-job TFLOP/s = world x steps x 6.67 n^3 / (max over ranks of device time)
              (work model: DBBR 4/3 n^3 + D&C <= 4/3 n^3 + back-transform 4 n^3)
-  e2e        the same metric through the C ABI with HOST buffers: every step copies A from
-             pinned host memory, solves, and copies eval + evec back
+  e2e        the same metric through the C ABI with HOST buffers (cuev_dsyevd_host): every step
+             copies A from pinned host memory, solves, and copies eval + evec back (the finished
+             eigenvector columns leave while the last columns' back-transform runs)
   roofline   the bulge-chasing back-transform kernel (2 n^3 FLOP over its column-range launches,
              timed from the first start to the last end) against the FP64 peak measured in the
              same run (cuBLAS DGEMM 8192^3)
@@ -377,9 +378,16 @@ def run_cuev(args, rank, world, local_rank):
         hA.copy_(A0.reshape(-1).cpu())
         hw = torch.empty(n, dtype=torch.float64, pin_memory=True)
         hV = torch.empty(n * n, dtype=torch.float64, pin_memory=True)
-        Af = A.reshape(-1)
-        Vf = V.reshape(-1)
         steps_e2e = max(1, min(args.steps, 2))
+
+        def solve_host():
+            # cuev_dsyevd_host: copy in, solve, eigenvectors copied out as they become final
+            st = lib.cuev_dsyevd_host(hA.data_ptr(), n, hw.data_ptr(), hV.data_ptr(), sp, None)
+            if st != 0:
+                raise RuntimeError(f"cuev_dsyevd_host failed: {st} "
+                                   f"{lib.cuev_last_error().decode()}")
+
+        solve_host()  # warm-up: the entry's device buffers are kept between calls
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
@@ -387,10 +395,7 @@ def run_cuev(args, rank, world, local_rank):
         for _ in range(steps_e2e):
             x0, x1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             x0.record(stream)
-            Af.copy_(hA, non_blocking=True)
-            solve()
-            hw.copy_(w, non_blocking=True)
-            hV.copy_(Vf, non_blocking=True)
+            solve_host()
             x1.record(stream)
             torch.cuda.synchronize()
             tot += x0.elapsed_time(x1)

@@ -82,6 +82,7 @@ _SIGS = {
     "cuev_dsyevd": [_DP, _I, _DP, _DP, _VP, C.POINTER(Timer)],
     "cuev_dsyevd_cfg": [_DP, _I, _DP, _DP, _VP, C.POINTER(Timer), C.POINTER(Config)],
     "cuev_ssyevd": [_FP, _I, _FP, _FP, _VP, C.POINTER(Timer)],
+    "cuev_dsyevd_host": [_VP, _I, _VP, _VP, _VP, C.POINTER(Timer)],
     "cuev_release_workspace": [],
     "cuev_handle_create": [_I, _I, _I, _VP, C.POINTER(C.c_void_p)],
     "cuev_handle_destroy": [_VP],
@@ -266,6 +267,26 @@ def eigh_batched(A_batch):
     _check(lib().cuev_dsyevd_batched(_ptr(Acm), n, bsz, _ptr(w), _ptr(Vcm),
                                      _stream(None)), "cuev_dsyevd_batched")
     return w, Vcm.transpose(1, 2)
+
+
+def eigh_host(A, evec: bool = True, stream=None, timer: Timer | None = None):
+    """Host-buffer solve (cuev_dsyevd_host): A is a (n, n) float64 array on the host, symmetric
+    (its lower triangle is read; a C-ordered array is the transpose, the same for a symmetric
+    matrix).  Returns (w, V) as host torch tensors (pinned), V column-major with eigenvectors as
+    columns (V[:, i] for w[i]); V is None when evec is False."""
+    import numpy as np
+    import torch
+    A_np = np.ascontiguousarray(np.asarray(A, dtype=np.float64))
+    n = A_np.shape[0]
+    if A_np.shape != (n, n):
+        raise ValueError("expected a square matrix")
+    hA = torch.from_numpy(A_np.T.copy()).pin_memory()          # column-major storage
+    w = torch.empty(n, dtype=torch.float64).pin_memory()
+    V = torch.empty(n * n, dtype=torch.float64).pin_memory() if evec else None
+    st = lib().cuev_dsyevd_host(hA.data_ptr(), n, w.data_ptr(), V.data_ptr() if evec else None,
+                                _stream(stream), C.byref(timer) if timer else None)
+    _check(st, "cuev_dsyevd_host")
+    return w, (V.view(n, n).t() if evec else None)
 
 
 def debug_set_wait_limit_ns(ns: int) -> None:

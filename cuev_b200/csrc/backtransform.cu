@@ -506,10 +506,15 @@ int back_transform(Workspace *ws, double *M, long long ldm, cudaEvent_t bc_end) 
     if (n > 2) CUEV_CHECK_STATUS(bc_back_prepare(ws, ws->stream));
     const int groups = div_up(std::max(n, 1), 32);
     const int full = groups / num_sms() * num_sms(); // groups in whole waves
+    // host-buffer entry: contiguous columns only (ld = n)
+    double *hV = (ws->host_evec && ldm == n) ? ws->host_evec : nullptr;
+    const size_t col_bytes = sizeof(double) * (size_t)n;
     if (n <= 2 || full == 0 || full == groups || !ws->side) {
         if (n > 2) CUEV_CHECK_STATUS(launch_bc_back_cols(ws, ws->stream, M, ldm, 0, n));
         if (bc_end) CUEV_TRY(cudaEventRecord(bc_end, ws->stream));
-        return sbr_back(ws, M, ldm);
+        CUEV_CHECK_STATUS(sbr_back(ws, M, ldm));
+        if (hV) CUEV_TRY(cudaMemcpyAsync(hV, M, col_bytes * n, cudaMemcpyDeviceToHost, ws->stream));
+        return CUEV_OK;
     }
     const int c1 = full * 32;
     CUEV_CHECK_STATUS(launch_bc_back_cols(ws, ws->stream, M, ldm, 0, c1));
@@ -520,8 +525,25 @@ int back_transform(Workspace *ws, double *M, long long ldm, cudaEvent_t bc_end) 
         st = CUEV_ERR_CUDA;
     if (st == CUEV_OK && cudaEventRecord(ws->ev_b, ws->side) != cudaSuccess) st = CUEV_ERR_CUDA;
     if (st == CUEV_OK) st = sbr_back_cols(ws, M, ldm, c1, ws->dc_T, ws->dc_Q2);
+    if (st == CUEV_OK && hV) {
+        // columns [0, c1) are final: copy them out on the side stream (after its BC-back) while
+        // the main stream computes the last columns
+        if (cudaEventRecord(ws->ev_c, ws->stream) != cudaSuccess ||
+            cudaStreamWaitEvent(ws->side, ws->ev_c, 0) != cudaSuccess ||
+            cudaMemcpyAsync(hV, M, col_bytes * c1, cudaMemcpyDeviceToHost, ws->side) !=
+                cudaSuccess ||
+            cudaEventRecord(ws->ev_d, ws->side) != cudaSuccess)
+            st = CUEV_ERR_CUDA;
+    }
     if (st == CUEV_OK && cudaStreamWaitEvent(ws->stream, ws->ev_b, 0) != cudaSuccess)
         st = CUEV_ERR_CUDA;
+    if (st == CUEV_OK) st = sbr_back_cols(ws, M + (long long)c1 * ldm, ldm, n - c1, ws->dc_T, ws->dc_Q2);
+    if (st == CUEV_OK && hV) {
+        if (cudaMemcpyAsync(hV + (size_t)c1 * n, M + (long long)c1 * ldm, col_bytes * (n - c1),
+                            cudaMemcpyDeviceToHost, ws->stream) != cudaSuccess ||
+            cudaStreamWaitEvent(ws->stream, ws->ev_d, 0) != cudaSuccess)
+            st = CUEV_ERR_CUDA;
+    }
     if (st != CUEV_OK) {
         // nothing of this call may outlive it on the side stream: join the side stream back into
         // the caller's stream (an event, not a host synchronisation, which would be illegal while
@@ -530,7 +552,7 @@ int back_transform(Workspace *ws, double *M, long long ldm, cudaEvent_t bc_end) 
             cudaStreamWaitEvent(ws->stream, ws->ev_b, 0);
         return st;
     }
-    return sbr_back_cols(ws, M + (long long)c1 * ldm, ldm, n - c1, ws->dc_T, ws->dc_Q2);
+    return CUEV_OK;
 }
 
 } // namespace cuev

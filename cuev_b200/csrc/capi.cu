@@ -124,8 +124,10 @@ struct MixedReq {
     bool fp32_bc_back = false; // FP32 entry: BC-back in FP32
 };
 
+// evec_host (optional, with evec): the eigenvectors are also copied there, the finished columns
+// while the back-transform's last columns are computed.
 int solve_d(double *A, int n, double *eval, double *evec, cudaStream_t stream, cuev_timer *timer,
-            const cuev_config *cfg, const MixedReq *mixed = nullptr) {
+            const cuev_config *cfg, const MixedReq *mixed = nullptr, double *evec_host = nullptr) {
     if (n < 0) return CUEV_ERR_INVALID;
     if (n == 0) return CUEV_OK;
     if (!A || !eval) return CUEV_ERR_INVALID; // evec == NULL: eigenvalues only
@@ -134,6 +136,8 @@ int solve_d(double *A, int n, double *eval, double *evec, cudaStream_t stream, c
     if (n == 1) {
         small_solve_kernel<<<1, 1, 0, stream>>>(A, eval, evec); note_launch();
         CUEV_TRY(cudaGetLastError());
+        if (evec && evec_host)
+            CUEV_TRY(cudaMemcpyAsync(evec_host, evec, sizeof(double), cudaMemcpyDeviceToHost, stream));
         CUEV_TRY(cudaStreamSynchronize(stream));
         if (timer) *timer = cuev_timer{};
         return CUEV_OK;
@@ -160,6 +164,11 @@ int solve_d(double *A, int n, double *eval, double *evec, cudaStream_t stream, c
     CUEV_TRY(cudaGetLastError());
     CUEV_CHECK_STATUS(workspace_check_status(ws, "input scan"));
 
+    struct HostFlag {
+        Workspace *ws;
+        ~HostFlag() { ws->host_evec = nullptr; }
+    } hflag{ws};
+    ws->host_evec = evec ? evec_host : nullptr;
     MixedFlag mflag{nullptr};
     if (mixed) {
         CUEV_CHECK_STATUS(workspace_enable_mixed(ws, mixed->refine));
@@ -233,7 +242,62 @@ struct WidenBuf {
     bool busy = false;
 };
 std::mutex g_wb_mu;
-WidenBuf g_wb[64];
+WidenBuf g_wb[64]; // FP32 entry
+WidenBuf g_hb[64]; // host-buffer entry
+
+// A cached per-device buffer of at least `need` bytes from `arr` (grown on demand), or, when it
+// is in use on another thread, a stream-ordered allocation (*cached = false).
+int devbuf_acquire(WidenBuf *arr, size_t need, cudaStream_t st, double **out, bool *cached,
+                   int *dev_out, const char *what) {
+    int dev = 0;
+    CUEV_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return CUEV_ERR_INVALID;
+    *dev_out = dev;
+    *out = nullptr;
+    *cached = false;
+    {
+        std::lock_guard<std::mutex> lk(g_wb_mu);
+        WidenBuf &wb = arr[dev];
+        if (!wb.busy) {
+            if (wb.bytes < need) {
+                if (wb.p) cudaFree(wb.p);
+                wb.p = nullptr;
+                wb.bytes = 0;
+                if (cudaMalloc((void **)&wb.p, need) == cudaSuccess) {
+                    wb.bytes = need;
+                } else {
+                    cudaGetLastError();
+                    wb.p = nullptr;
+                }
+            }
+            if (wb.p) {
+                wb.busy = true;
+                *out = wb.p;
+                *cached = true;
+            }
+        }
+    }
+    if (!*out && cudaMallocAsync((void **)out, need, st) != cudaSuccess) {
+        cudaGetLastError();
+        *out = nullptr;
+        char msg[128];
+        snprintf(msg, sizeof(msg), "%s: device buffer allocation failed", what);
+        set_last_message(msg);
+        return CUEV_ERR_ALLOC;
+    }
+    return CUEV_OK;
+}
+
+// Give back a buffer from devbuf_acquire; the stream must be synchronised for a cached one.
+void devbuf_release(WidenBuf *arr, int dev, double *p, bool cached, cudaStream_t st) {
+    if (!p) return;
+    if (!cached) {
+        cudaFreeAsync(p, st);
+        return;
+    }
+    std::lock_guard<std::mutex> lk(g_wb_mu);
+    arr[dev].busy = false;
+}
 
 __global__ void widen_kernel(const float *__restrict__ s, double *__restrict__ d, long long cnt) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < cnt;
@@ -280,37 +344,9 @@ extern "C" int cuev_ssyevd(float *A, int n, float *eval, float *evec, void *stre
     const long long nn = (long long)n * n;
     const size_t need = sizeof(double) * (2 * nn + n);
     int dev = 0;
-    CUEV_TRY(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= 64) return CUEV_ERR_INVALID;
     double *buf = nullptr;
     bool cached = false;
-    {
-        std::lock_guard<std::mutex> lk(g_wb_mu);
-        WidenBuf &wb = g_wb[dev];
-        if (!wb.busy) {
-            if (wb.bytes < need) {
-                if (wb.p) cudaFree(wb.p);
-                wb.p = nullptr;
-                wb.bytes = 0;
-                if (cudaMalloc((void **)&wb.p, need) == cudaSuccess) {
-                    wb.bytes = need;
-                } else {
-                    cudaGetLastError();
-                    wb.p = nullptr;
-                }
-            }
-            if (wb.p) {
-                wb.busy = true;
-                buf = wb.p;
-                cached = true;
-            }
-        }
-    }
-    if (!buf && cudaMallocAsync((void **)&buf, need, st) != cudaSuccess) {
-        cudaGetLastError();
-        set_last_message("FP32 entry: widening buffer allocation failed");
-        return CUEV_ERR_ALLOC;
-    }
+    CUEV_CHECK_STATUS(devbuf_acquire(g_wb, need, st, &buf, &cached, &dev, "FP32 entry"));
     double *A64 = buf, *V64 = buf + nn, *w64 = buf + 2 * nn;
     const int blocks = 4 * num_sms();
     widen_kernel<<<blocks, 256, 0, st>>>(A, A64, nn); note_launch();
@@ -325,12 +361,36 @@ extern "C" int cuev_ssyevd(float *A, int n, float *eval, float *evec, void *stre
         narrow_kernel<<<1, 256, 0, st>>>(w64, eval, n); note_launch();
         narrow_kernel<<<blocks, 256, 0, st>>>(A64, A, nn); note_launch(); // A is clobbered like the reference's
     }
-    if (!cached) cudaFreeAsync(buf, st);
+    if (!cached) devbuf_release(g_wb, dev, buf, false, st);
     if (cudaStreamSynchronize(st) != cudaSuccess && s == CUEV_OK) s = CUEV_ERR_CUDA;
-    if (cached) {
-        std::lock_guard<std::mutex> lk(g_wb_mu);
-        g_wb[dev].busy = false;
-    }
+    if (cached) devbuf_release(g_wb, dev, buf, true, st);
+    return s;
+}
+
+extern "C" int cuev_dsyevd_host(const double *A_host, int n, double *eval_host,
+                                double *evec_host, void *stream, cuev_timer *timer) {
+    if (n < 0) return CUEV_ERR_INVALID;
+    if (n == 0) return CUEV_OK;
+    if (!A_host || !eval_host) return CUEV_ERR_INVALID;
+    cudaStream_t st = (cudaStream_t)stream;
+    const long long nn = (long long)n * n;
+    const size_t need = sizeof(double) * ((evec_host ? 2 * nn : nn) + n);
+    int dev = 0;
+    double *buf = nullptr;
+    bool cached = false;
+    CUEV_CHECK_STATUS(devbuf_acquire(g_hb, need, st, &buf, &cached, &dev, "host-buffer entry"));
+    double *dA = buf, *dw = buf + nn, *dV = evec_host ? buf + nn + n : nullptr;
+    int s = CUEV_OK;
+    if (cudaMemcpyAsync(dA, A_host, sizeof(double) * nn, cudaMemcpyHostToDevice, st) != cudaSuccess)
+        s = CUEV_ERR_CUDA;
+    // the eigenvectors reach evec_host inside the solve (copied out column block by column block)
+    if (s == CUEV_OK) s = solve_d(dA, n, dw, dV, st, timer, nullptr, nullptr, evec_host);
+    if (s == CUEV_OK &&
+        cudaMemcpyAsync(eval_host, dw, sizeof(double) * n, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+        s = CUEV_ERR_CUDA;
+    if (!cached) devbuf_release(g_hb, dev, buf, false, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess && s == CUEV_OK) s = CUEV_ERR_CUDA;
+    if (cached) devbuf_release(g_hb, dev, buf, true, st);
     return s;
 }
 
@@ -346,12 +406,13 @@ extern "C" int cuev_release_workspace(void) {
         std::lock_guard<std::mutex> lk(cuev::g_wb_mu);
         int cur = 0;
         if (cudaGetDevice(&cur) == cudaSuccess) {
-            for (int d = 0; d < 64; ++d)
-                if (cuev::g_wb[d].p && !cuev::g_wb[d].busy) {
-                    if (cudaSetDevice(d) == cudaSuccess) cudaFree(cuev::g_wb[d].p);
-                    cuev::g_wb[d].p = nullptr;
-                    cuev::g_wb[d].bytes = 0;
-                }
+            for (cuev::WidenBuf *arr : {cuev::g_wb, cuev::g_hb})
+                for (int d = 0; d < 64; ++d)
+                    if (arr[d].p && !arr[d].busy) {
+                        if (cudaSetDevice(d) == cudaSuccess) cudaFree(arr[d].p);
+                        arr[d].p = nullptr;
+                        arr[d].bytes = 0;
+                    }
             cudaSetDevice(cur);
         }
         cudaGetLastError();

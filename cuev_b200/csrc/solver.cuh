@@ -28,6 +28,11 @@ struct Workspace {
     // partial wave with the SBR-back of the columns already finished
     cudaStream_t side = nullptr;
     cudaEvent_t ev_a = nullptr, ev_b = nullptr;
+    // host-buffer entry: while host_evec is set, the back-transform copies the finished
+    // eigenvector columns to it (the whole waves' columns on the side stream while the last
+    // columns are still being computed; ev_c / ev_d order those copies)
+    double *host_evec = nullptr;
+    cudaEvent_t ev_c = nullptr, ev_d = nullptr;
 
     double *Y = nullptr, *Z = nullptr, *Wp = nullptr, *Tp = nullptr, *Tblk = nullptr;
     double *tau = nullptr, *Dwk = nullptr, *Cwk = nullptr, *Gblk = nullptr;

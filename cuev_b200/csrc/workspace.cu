@@ -89,7 +89,9 @@ int workspace_create(int n, int b, int k, cudaStream_t stream, Workspace **out) 
     if (cudaDeviceGetStreamPriorityRange(&least, &greatest) != cudaSuccess ||
         cudaStreamCreateWithPriority(&ws->side, cudaStreamNonBlocking, greatest) != cudaSuccess ||
         cudaEventCreateWithFlags(&ws->ev_a, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&ws->ev_b, cudaEventDisableTiming) != cudaSuccess) {
+        cudaEventCreateWithFlags(&ws->ev_b, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ws->ev_c, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ws->ev_d, cudaEventDisableTiming) != cudaSuccess) {
         cudaGetLastError();
         workspace_destroy(ws);
         set_last_message("workspace: stream or event creation failed");
@@ -156,6 +158,8 @@ void workspace_destroy(Workspace *ws) {
     if (ws->side) cudaStreamSynchronize(ws->side), cudaStreamDestroy(ws->side);
     if (ws->ev_a) cudaEventDestroy(ws->ev_a);
     if (ws->ev_b) cudaEventDestroy(ws->ev_b);
+    if (ws->ev_c) cudaEventDestroy(ws->ev_c);
+    if (ws->ev_d) cudaEventDestroy(ws->ev_d);
     if (ws->pool) cudaFree(ws->pool);
     delete ws;
 }

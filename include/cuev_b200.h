@@ -72,6 +72,16 @@ int cuev_dsyevd(double *A, int n, double *eval, double *evec, void *stream, cuev
 int cuev_dsyevd_cfg(double *A, int n, double *eval, double *evec, void *stream, cuev_timer *timer,
                     const cuev_config *cfg);
 
+/* Host-buffer form of cuev_dsyevd (no reference counterpart: the reference takes device
+ * pointers): A_host (n x n column-major, lower triangle read, not modified), eval_host (n) and
+ * evec_host (n x n, or NULL for eigenvalues only) in host memory (pinned for full copy speed).
+ * A is copied in, solved on `stream`, and the eigenvector columns are copied out as they become
+ * final (the columns of BC-back's whole waves while the last columns' back-transform runs).
+ * Device buffers ((2 n^2 + n) doubles) are kept per device between calls and released by
+ * cuev_release_workspace.  Blocks until done. */
+int cuev_dsyevd_host(const double *A_host, int n, double *eval_host, double *evec_host,
+                     void *stream, cuev_timer *timer);
+
 /* FP32 interface.  Replaces cuev::symm_eig_solve<float> (reference src/cuda/solver.cu:78).
  * The float input is widened and solved by the FP64 band reduction, bulge chase and D&C; BC-back
  * runs in FP32 (b = 32; on float copies of the reflectors and eigenvectors, n^2 floats each, kept
@@ -158,8 +168,8 @@ int cuev_dsyevd_mixed(double *A, int n, double *eval, double *evec, void *stream
                       cuev_mixed_info *info);
 
 /* Release the cached device workspace (the solves keep one pool per (n, b, k) between calls, the
- * batched eigensolver one buffer per device for 64 < n <= 512, the FP32 entry one widening buffer
- * per device, (2 n^2 + n) doubles). */
+ * batched eigensolver one buffer per device for 64 < n <= 512, the FP32 and host-buffer entries
+ * one buffer each per device, (2 n^2 + n) doubles). */
 int cuev_release_workspace(void);
 
 /* Message for the last failing call on this host thread ("" if none). */

@@ -184,6 +184,28 @@ def test_fp32_entry(cuda, n):
     assert np.linalg.norm(Vn.T @ Vn - np.eye(n)) / np.sqrt(n) < 1e-5
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [1, 300, 5000])
+def test_host_entry(cuda, n):
+    """cuev_dsyevd_host copies A in, solves and copies the eigenvectors out as they become final
+    (at n = 5000 the columns of BC-back's whole waves leave while the last columns are computed);
+    the results are the device entry's, bit for bit."""
+    import torch
+    import cuev_b200 as cv
+    A = _sym(n, 11)
+    w_h, V_h = cv.eigh_host(A)
+    dA = torch.from_numpy(np.asfortranarray(A).ravel(order="F").copy()).to(cuda)
+    w = torch.zeros(n, dtype=torch.float64, device=cuda)
+    V = torch.zeros(n * n, dtype=torch.float64, device=cuda)
+    cv.symm_eig_solve(dA, n, w, V)
+    torch.cuda.synchronize()
+    assert np.array_equal(w_h.numpy(), w.cpu().numpy())
+    assert np.array_equal(V_h.t().contiguous().numpy().ravel(), V.cpu().numpy())
+    w2, V2 = cv.eigh_host(A, evec=False)                      # eigenvalues only (bisection)
+    assert V2 is None
+    assert np.abs(w2.numpy() - w_h.numpy()).max() <= 1e-12 * max(1.0, np.abs(w_h.numpy()).max())
+
+
 def test_error_codes(cuda):
     import torch
     import cuev_b200 as cv
