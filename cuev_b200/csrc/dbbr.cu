@@ -598,12 +598,15 @@ int dbbr_reduce(Workspace *ws, double *A) {
             CUEV_CHECK_STATUS(
                 ws_gemm(ws, 0, 0, rows, b, b, -0.5, Ypan, ld, ws->Cwk, b, 1.0, Zcur, ld));
             w += b;
-            // green update of the next panel's columns: A[j+b:, j+b:j+2b] -= Z Yg^T + Y Zg^T
+            // green update of the next panel's columns: A[j+b:, j+b:j+b+nb] -= Z Yg^T + Y Zg^T,
+            // nb = b except at the end of the matrix, where the last columns number fewer than b
+            // (n not a multiple of b): the update must stop at column n - 1
             if (j + b < i + kc) {
-                const double *Yg = Y + (long long)i * ld + (j + b); // Y[j+b:j+2b, i:i+w]
-                const double *Zg = Z + (j + b);                     // Z[j+b:j+2b, 0:w]
-                CUEV_CHECK_STATUS(ws_gemm2(ws, 0, 1, rows, b, w, w, -1.0, Zblk, ld, Yblk, ld, Yg, ld,
-                                           Zg, ld, 1.0, Atr, ld, 0));
+                const int nb = std::min(b, rows);
+                const double *Yg = Y + (long long)i * ld + (j + b); // Y[j+b:j+b+nb, i:i+w]
+                const double *Zg = Z + (j + b);                     // Z[j+b:j+b+nb, 0:w]
+                CUEV_CHECK_STATUS(ws_gemm2(ws, 0, 1, rows, nb, w, w, -1.0, Zblk, ld, Yblk, ld, Yg,
+                                           ld, Zg, ld, 1.0, Atr, ld, 0));
             }
         }
         // aggregated WY factor of the block for the back-transform:

@@ -115,13 +115,14 @@ def test_config2_full_size(cuda, nbw):
     assert orth < 1e-13, orth
 
 
-@pytest.mark.parametrize("n", [4740, 4768])
-def test_backtransform_overlap_last_group(cuda, n):
-    """The back-transform's BC-back grid at n = 4740 / 4768 is 148 groups of 32 columns (one whole
-    wave on 148 SMs) plus one group 4 / 32 columns wide: the whole wave runs first, then the
-    one-CTA last wave beside the SBR-back of the first 4736 columns, then the SBR-back of the last
-    columns.  Every column must come out right: residual and orthogonality over all of V, and the
-    eigenvalues against the eigenvalues-only path (bisection, no back-transform)."""
+@pytest.mark.parametrize("n,nbw", [(4740, 32), (4768, 32), (2372, 64), (2384, 64)])
+def test_backtransform_overlap_last_group(cuda, n, nbw):
+    """The back-transform's BC-back grid at n = 4740 / 4768 (b = 32) is 148 groups of 32 columns
+    (one whole wave on 148 SMs) plus one group 4 / 32 columns wide, and at n = 2372 / 2384
+    (b = 64, 16 columns per CTA) 148 groups of 16 plus one of 4 / 16: the whole wave runs first,
+    then the one-CTA last wave beside the SBR-back of the first columns, then the SBR-back of the
+    last columns.  Every column must come out right: residual and orthogonality over all of V, and
+    the eigenvalues against the eigenvalues-only path (bisection, no back-transform)."""
     import torch
     import cuev_b200 as cv
     g = torch.Generator(device=cuda).manual_seed(n)
@@ -130,10 +131,10 @@ def test_backtransform_overlap_last_group(cuda, n):
     del G
     A0 = A.clone()
     w_bis = torch.zeros(n, dtype=torch.float64, device=cuda)
-    cv.symm_eig_solve(A0.clone(), n, w_bis, None, nbw=32, nk=256)
+    cv.symm_eig_solve(A0.clone(), n, w_bis, None, nbw=nbw, nk=256)
     w = torch.zeros(n, dtype=torch.float64, device=cuda)
     V = torch.zeros(n, n, dtype=torch.float64, device=cuda)
-    cv.symm_eig_solve(A, n, w, V, nbw=32, nk=256)
+    cv.symm_eig_solve(A, n, w, V, nbw=nbw, nk=256)
     torch.cuda.synchronize()
     anorm = float(w_bis.abs().max())
     dl = float((w - w_bis).abs().max()) / anorm
@@ -148,6 +149,44 @@ def test_backtransform_overlap_last_group(cuda, n):
     assert resid < 1e-13, resid
     assert worst_col < 1e-11, worst_col
     assert orth < 1e-13, orth
+
+
+@pytest.mark.parametrize("n,nbw,nk", [(4740, 32, 256), (777, 32, 128), (100, 32, 256),
+                                      (1500, 64, 256), (131, 64, 128)])
+def test_no_access_past_the_matrix(cuda, n, nbw, nk):
+    """n not a multiple of b: the band reduction's last panel update covers fewer than b columns
+    and must stop at column n - 1.  A (and V, w) sit at the front of larger device buffers filled
+    with a sentinel; after the full solve and the eigenvalues-only solve every sentinel is intact
+    (writes past the matrix would change them) and the results are right."""
+    import torch
+    import cuev_b200 as cv
+    A = _sym(n, n + 5)
+    pad = 64 * n + 4096
+    sent = 12345.0
+
+    def padded(numel, init=None):
+        buf = torch.full((numel + pad,), sent, dtype=torch.float64, device=cuda)
+        if init is not None:
+            buf[:numel] = init
+        return buf
+
+    a_col = torch.from_numpy(np.asfortranarray(A).ravel(order="F").copy()).to(cuda)
+    for evec in (True, False):
+        bA = padded(n * n, a_col)
+        bw = padded(n)
+        bV = padded(n * n) if evec else None
+        cv.symm_eig_solve(bA[: n * n], n, bw[:n], bV[: n * n] if evec else None, nbw=nbw, nk=nk)
+        torch.cuda.synchronize()
+        for buf, numel in ((bA, n * n), (bw, n)) + (((bV, n * n),) if evec else ()):
+            tail = buf[numel:]
+            assert bool((tail == sent).all()), int((tail != sent).sum())
+        w = bw[:n].cpu().numpy()
+        w_ref = np.linalg.eigvalsh(A)
+        assert np.abs(w - w_ref).max() / np.abs(w_ref).max() < 1e-12
+        if evec:
+            V = bV[: n * n].cpu().numpy().reshape((n, n)).T
+            resid = np.linalg.norm(A @ V - V * w) / (n * np.abs(w_ref).max())
+            assert resid < 1e-13, resid
 
 
 def test_timer_and_reuse(cuda):

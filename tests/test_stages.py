@@ -102,7 +102,8 @@ def test_bc_chase_vs_oracle(cuda, n, b):
 
 
 @pytest.mark.parametrize("n,b,k", [(256, 32, 128), (384, 32, 128), (777, 32, 128),
-                                   (1024, 32, 128), (1000, 64, 512)])
+                                   (1024, 32, 128), (1000, 64, 512), (130, 64, 128),
+                                   (777, 64, 128)])
 def test_backtransform_vs_oracle(cuda, n, b, k):
     """Q_b and Q_s materialised by applying the GPU back-transform to I (the reference's
     test_backtransform.cu:162-215), checked against the oracle applied to the same reflectors
