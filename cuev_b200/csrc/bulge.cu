@@ -32,22 +32,25 @@
 namespace cuev {
 namespace {
 
-constexpr int BC_THREADS = 256;
+// Threads per hop.  b = 64's window (2b x 3b) is four times b = 32's, so it runs twice the threads
+// (n = 16384, b = 64: 355 -> 286 ms; n = 8192: 174 -> 140 ms).  At b = 32 the hop is bound by its
+// L2 round trips and fences, not its arithmetic: 384 and 512 threads measured the same as 256.
+template <int BW> constexpr int chase_threads() { return BW == 64 ? 512 : 256; }
 
 template <int BW> struct ChaseSmem {
     double S[BW][3 * BW + 1]; // strip: S[k][ii] = A(lo + ii, r0 + k)
     double w[BW];             // reflector
     double p[3 * BW];         // p = 2 A w over the window rows
     double beta;
-    double kap[BC_THREADS / 32]; // per-warp partial sums of kappa = w^T p
+    double kap[chase_threads<BW>() / 32]; // per-warp partial sums of kappa = w^T p
 };
 
 template <int BW>
-__global__ void __launch_bounds__(BC_THREADS)
+__global__ void __launch_bounds__(chase_threads<BW>())
     bc_chase_kernel(double *__restrict__ Bp, double *__restrict__ U, long long ldu, int n, int b,
                     int *prog, int *status) {
     int *prog_ref = prog + n; // per sweep: cq of the last hop whose beta is in the band
-    constexpr int NT = BC_THREADS;
+    constexpr int NT = chase_threads<BW>();
     constexpr int NLEFT = (BW * BW + NT - 1) / NT;    // left-block elements per thread
     constexpr int NLOW = (2 * BW * BW + NT - 1) / NT; // lower-part elements per thread
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -181,7 +184,8 @@ __global__ void __launch_bounds__(BC_THREADS)
             // diagonal block read from its mirror), and per-warp partial sums of
             // kappa = w^T p over the reflector rows (rows off .. off + L - 1)
             {
-                constexpr int TPR = (NT >= 2 * 3 * BW) ? 2 : 1;
+                // threads per row: as many (4, 2 or 1) as leave the last warp without a row
+                constexpr int TPR = (NT > 4 * 3 * BW + 31) ? 4 : (NT > 2 * 3 * BW + 31) ? 2 : 1;
                 constexpr int KP = BW / TPR;                 // k range per thread
                 constexpr int PW = (3 * BW * TPR + 31) / 32; // warps that hold rows
                 static_assert(PW < NT / 32, "the last warp holds no row");
@@ -216,7 +220,8 @@ __global__ void __launch_bounds__(BC_THREADS)
                         for (; k < k1; ++k) a0 = fma(sm.S[k][ii], sm.w[k], a0);
                     }
                     double pr = (a0 + a1) + (a2 + a3);
-                    if constexpr (TPR == 2) pr += __shfl_xor_sync(0xffffffffu, pr, 1);
+#pragma unroll
+                    for (int o = 1; o < TPR; o <<= 1) pr += __shfl_xor_sync(0xffffffffu, pr, o);
                     pr *= 2.0;
                     if (act && h == 0) {
                         sm.p[ii] = pr;
@@ -302,7 +307,7 @@ template <int BW> int launch_chase(Workspace *ws, double *B) {
     auto kern = bc_chase_kernel<BW>;
     CUEV_CHECK_STATUS(ensure_dyn_smem((const void *)kern, smem));
     int per_sm = 0;
-    CUEV_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, BC_THREADS, smem));
+    CUEV_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, chase_threads<BW>(), smem));
     // at most two CTAs per SM: a hop's latency grows with the CTAs that share its SM, and two per
     // SM still keep more sweeps in flight than the wavefront needs (n = 16384: 3 per SM 179.7 ms,
     // 2 per SM 175.6, 1 per SM 176.1)
@@ -313,7 +318,7 @@ template <int BW> int launch_chase(Workspace *ws, double *B) {
     int nn = n, bb = b;
     void *args[] = {&B, &U, &ldu, &nn, &bb, &ws->prog, &ws->status};
     note_launch();
-    CUEV_TRY(cudaLaunchCooperativeKernel((void *)kern, dim3(grid), dim3(BC_THREADS), args, smem,
+    CUEV_TRY(cudaLaunchCooperativeKernel((void *)kern, dim3(grid), dim3(chase_threads<BW>()), args, smem,
                                          ws->stream));
     return CUEV_OK;
 }

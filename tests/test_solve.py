@@ -189,6 +189,34 @@ def test_no_access_past_the_matrix(cuda, n, nbw, nk):
             assert resid < 1e-13, resid
 
 
+@pytest.mark.parametrize("entry", ["fp32", "mixed"])
+def test_no_access_past_the_buffers_other_entries(cuda, entry):
+    """The FP32 entry and the precision form at n = 1001 (not a multiple of 32): the caller's
+    A, w and V sit at the front of sentinel-filled buffers, which must come back intact."""
+    import torch
+    import cuev_b200 as cv
+    n = 1001
+    A = _sym(n, 17)
+    dt = torch.float32 if entry == "fp32" else torch.float64
+    pad = 64 * n + 4096
+    sent = 12345.0
+    a_col = torch.from_numpy(np.asfortranarray(A).ravel(order="F").copy()).to(cuda, dt)
+    bufs = [torch.full((numel + pad,), sent, dtype=dt, device=cuda) for numel in (n * n, n, n * n)]
+    bA, bw, bV = bufs
+    bA[: n * n] = a_col
+    if entry == "fp32":
+        cv.symm_eig_solve(bA[: n * n], n, bw[:n], bV[: n * n])
+    else:
+        cv.symm_eig_solve_mixed(bA[: n * n], n, bw[:n], bV[: n * n])
+    torch.cuda.synchronize()
+    for buf, numel in zip(bufs, (n * n, n, n * n)):
+        assert bool((buf[numel:] == sent).all()), int((buf[numel:] != sent).sum())
+    w = bw[:n].double().cpu().numpy()
+    w_ref = np.linalg.eigvalsh(A)
+    tol = 1e-5 if entry == "fp32" else 1e-12
+    assert np.abs(w - w_ref).max() / np.abs(w_ref).max() < tol
+
+
 def test_timer_and_reuse(cuda):
     import cuev_b200 as cv
     A = _sym(600, 3)
