@@ -44,19 +44,21 @@ def test_solve_waits_time_out_then_next_solve_succeeds(cuda):
     assert m["max_dlambda_rel"] < 1e-12 and m["resid_n_norm2"] < 1e-13, m
 
 
-def test_bc_back_pipeline_waits_time_out_then_recover(cuda):
+@pytest.mark.parametrize("nbw", [32, 64])
+def test_bc_back_pipeline_waits_time_out_then_recover(cuda, nbw):
     """Stage entries: the first stages run with the normal bound; the back-transform (BC-back's
-    warp pipeline waits on shared-memory counters of its neighbour warps) then runs with a 1 ns
-    bound and must report the timeout; rerun with the normal bound it must be exact again."""
+    warp pipeline waits on shared-memory counters of its neighbour warps; at b = 64 each wait is
+    decided by a vote of the warp's lanes) then runs with a 1 ns bound and must report the
+    timeout; rerun with the normal bound it must be exact again."""
     import torch
     import cuev_b200 as cv
     n = 1024
     A = _sym(n, 77)
     w_ref = np.linalg.eigvalsh(A)
-    with cv.SolverHandle(n, nbw=32, nk=256) as h:
+    with cv.SolverHandle(n, nbw=nbw, nk=256) as h:
         dA = torch.from_numpy(A.ravel(order="F").copy()).cuda()
         h.dbbr_reduce(dA)
-        B, _ = h.buffer(cv.BUF_B, 64, n)
+        B, _ = h.buffer(cv.BUF_B, 2 * nbw, n)
         d = torch.zeros(n, dtype=torch.float64, device="cuda")
         e = torch.zeros(n, dtype=torch.float64, device="cuda")
         h.bc_chase(B, d, e)
