@@ -583,20 +583,34 @@ int dbbr_reduce(Workspace *ws, double *A) {
             // panel QR -> R (in A), Y, tau, T, W = Y T
             CUEV_CHECK_STATUS(
                 panel_qr(ws, Apan, ld, Ypan, ld, ws->tau + j, Tpan, Wpan, ld, rows, b));
-            // P = A_trail W (A_trail symmetric, lower triangle, not yet updated for this block)
+            // P0 = A_trail W (A_trail symmetric, lower triangle, not yet updated for this block)
             CUEV_CHECK_STATUS(ws_symm(ws, rows, b, 1.0, Atr, ld, Wpan, ld, 0.0, Zcur, ld));
+            // The panel's Z, in the order of the reference (dbbr.cu:175-198):
+            //   P = P0 - Y_blk D1 - Z_blk D2,  D1 = Z_blk^T W,  D2 = Y_blk^T W,
+            //   C = W^T P,  Z = P - 1/2 Y_pan C.
+            // Here with two dependent products fewer.  W^T P expands to
+            // G - D2^T D1 - D1^T D2 (G = W^T P0), so C needs no pass over P; Z_cur sits right
+            // after Z_blk in Z and Y_pan right after Y_blk in Y, so one product gives
+            // E = [Z_blk | P0]^T W = [D1; G^T] and one two-segment product gives
+            //   Z = P0 - [Y_blk | Y_pan] [D1; C^T / 2] - Z_blk D2.
+            // C is symmetric in exact arithmetic; its transpose differs by rounding only.
+            const int le = w + b;
+            double *E = ws->Dwk;                        // (w + b) x b, ld w + b
+            double *D2 = ws->Dwk + (size_t)k * b;       // w x b, ld w
+            const double *ZP = Z + (j + b);             // Z[j+b:, 0:w+b] = [Z_blk | Z_cur]
+            CUEV_CHECK_STATUS(ws_gemm(ws, 1, 0, le, b, rows, 1.0, ZP, ld, Wpan, ld, 0.0, E, le));
             if (w > 0) {
-                // D1 = Z_blk^T W, D2 = Y_blk^T W ;  P -= Y_blk D1 + Z_blk D2
-                double *D1 = ws->Dwk, *D2 = ws->Dwk + (size_t)k * b;
-                CUEV_CHECK_STATUS(ws_gemm(ws, 1, 0, w, b, rows, 1.0, Zblk, ld, Wpan, ld, 0.0, D1, w));
                 CUEV_CHECK_STATUS(ws_gemm(ws, 1, 0, w, b, rows, 1.0, Yblk, ld, Wpan, ld, 0.0, D2, w));
-                CUEV_CHECK_STATUS(ws_gemm2(ws, 0, 0, rows, b, w, w, -1.0, Yblk, ld, Zblk, ld, D1, w,
+                // E[w:w+b] = (G^T - D1^T D2 - D2^T D1) / 2 = C^T / 2
+                CUEV_CHECK_STATUS(ws_gemm2(ws, 1, 0, b, b, w, w, -0.5, E, le, D2, w, D2, w, E, le,
+                                           0.5, E + w, le, 0));
+                const double *YP = Y + (long long)i * ld + (j + b); // [Y_blk | Y_pan]
+                CUEV_CHECK_STATUS(ws_gemm2(ws, 0, 0, rows, b, le, w, -1.0, YP, ld, Zblk, ld, E, le,
                                            D2, w, 1.0, Zcur, ld, 0));
+            } else {
+                // first panel of the block: E = G^T, Z = P0 - 1/2 Y_pan G^T
+                CUEV_CHECK_STATUS(ws_gemm(ws, 0, 0, rows, b, b, -0.5, Ypan, ld, E, le, 1.0, Zcur, ld));
             }
-            // C = W^T P (b x b) ;  Z = P - 1/2 Y C
-            CUEV_CHECK_STATUS(ws_gemm(ws, 1, 0, b, b, rows, 1.0, Wpan, ld, Zcur, ld, 0.0, ws->Cwk, b));
-            CUEV_CHECK_STATUS(
-                ws_gemm(ws, 0, 0, rows, b, b, -0.5, Ypan, ld, ws->Cwk, b, 1.0, Zcur, ld));
             w += b;
             // green update of the next panel's columns: A[j+b:, j+b:j+b+nb] -= Z Yg^T + Y Zg^T,
             // nb = b except at the end of the matrix, where the last columns number fewer than b

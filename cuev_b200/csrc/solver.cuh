@@ -35,7 +35,7 @@ struct Workspace {
     cudaEvent_t ev_c = nullptr, ev_d = nullptr;
 
     double *Y = nullptr, *Z = nullptr, *Wp = nullptr, *Tp = nullptr, *Tblk = nullptr;
-    double *tau = nullptr, *Dwk = nullptr, *Cwk = nullptr, *Gblk = nullptr;
+    double *tau = nullptr, *Dwk = nullptr, *Gblk = nullptr;
     double *B = nullptr, *U = nullptr, *d = nullptr, *e = nullptr;
     int *prog = nullptr; // 2n words: bulge-chase progress per sweep (hops done, betas written)
     unsigned *bar = nullptr; // grid-barrier words for cooperative kernels

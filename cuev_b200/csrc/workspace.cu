@@ -54,7 +54,6 @@ int workspace_create(int n, int b, int k, cudaStream_t stream, Workspace **out) 
         {(void **)&ws->Tblk, (N / k + 2) * (size_t)k * k * s},
         {(void **)&ws->tau, (N + 64) * s},
         {(void **)&ws->Dwk, 2 * (size_t)k * b * s},
-        {(void **)&ws->Cwk, (size_t)b * b * s},
         {(void **)&ws->Gblk, (size_t)k * k * s},
         {(void **)&ws->B, 2 * (size_t)b * N * s},
         {(void **)&ws->d, N * s},
