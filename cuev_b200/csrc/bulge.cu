@@ -63,25 +63,29 @@ __global__ void __launch_bounds__(chase_threads<BW>())
 
     for (int s = blockIdx.x; s < nsweeps; s += gridDim.x) {
         for (int hop = 0;; ++hop) {
-            int cq, r0, r1;
+            int cq, r0, r1u; // r1u: last reflector row before clipping to the matrix
             if (hop == 0) {
-                cq = s, r0 = s + 1, r1 = min(s + b, n - 1);
+                cq = s, r0 = s + 1, r1u = s + b;
             } else {
                 const int c = s + 1 + (hop - 1) * b;
                 if (c + b >= n) break;
-                cq = c, r0 = c + b, r1 = min(c + 2 * b - 1, n - 1);
+                cq = c, r0 = c + b, r1u = c + 2 * b - 1;
             }
+            const int r1 = min(r1u, n - 1);
             const int L = r1 - r0 + 1;
             const int lo = cq, hi = min(n - 1, r1 + b);
             const int W = hi - lo + 1;
             const int off = r0 - lo; // strip row of reflector row r0
 
-            // ---- wait for sweep s-1: every hop that starts at or before r1 - b completed, and
-            // the beta of the hop that starts in (r1 - b, r1] written
+            // ---- wait for sweep s-1: every hop that starts at or before r1u - b completed, and
+            // the beta of the hop that starts in (r1u - b, r1u] written.  The thresholds come from
+            // the unclipped r1u: at the end of the matrix sweep s-1 has no hop that far on, so
+            // the wait runs to its end-of-sweep release (with the clipped r1 the thresholds fall
+            // below the counters' initial -1 when n <= b, and nothing would be waited for).
             if (tid == 0) {
                 int ok = 1;
                 if (s > 0) {
-                    const int need = r1 - b + 1;
+                    const int need = r1u - b + 1;
                     const uint64_t t0 = global_ns();
                     const uint64_t limit = wait_limit_ns(status);
                     // the clock is read every 256 polls, or every poll under a short limit

@@ -32,6 +32,9 @@ def _sym(n, seed):
 @pytest.mark.parametrize("n,nbw,nk", [(2, 32, 256), (3, 32, 256), (33, 32, 256), (65, 32, 256),
                                       (100, 32, 256), (257, 32, 128), (777, 32, 128),
                                       (1024, 32, 256), (1024, 64, 512), (1500, 64, 256),
+                                      (2, 64, 128), (3, 64, 128), (40, 64, 128), (65, 64, 128),
+                                      (100, 64, 128), (130, 64, 128), (20, 32, 128),
+                                      (31, 32, 128), (32, 32, 128), (63, 64, 128), (64, 64, 128),
                                       (2048, 0, 0)])
 def test_solve_vs_dsyevd(cuda, n, nbw, nk):
     A = _sym(n, n + nbw)

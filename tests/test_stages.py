@@ -74,8 +74,11 @@ def test_dbbr_reduce_vs_oracle(cuda, n, b, k):
     assert np.abs(ev - ev_ref).max() / (ev_ref[-1] - ev_ref[0]) < 1e-9
 
 
-@pytest.mark.parametrize("n,b", [(256, 64), (512, 64), (513, 32), (1024, 32), (2000, 64)])
+@pytest.mark.parametrize("n,b", [(256, 64), (512, 64), (513, 32), (1024, 32), (2000, 64),
+                                 (20, 32), (32, 32), (40, 64), (64, 64)])
 def test_bc_chase_vs_oracle(cuda, n, b):
+    """n <= b included: every sweep is then a single hop clipped at the matrix end, and each
+    must wait for the previous sweep to finish."""
     import torch
     import cuev_b200 as cv
     rng = np.random.default_rng(n + b)
