@@ -82,7 +82,8 @@ def test_tridi_eigvals_stage(cuda, case):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("n,nbw", [(1, 32), (2, 32), (3, 32), (257, 32), (2048, 32), (1024, 64)])
+@pytest.mark.parametrize("n,nbw", [(1, 32), (2, 32), (3, 32), (20, 32), (257, 32), (2048, 32),
+                                   (40, 64), (300, 64), (1024, 64)])
 def test_eigvals_only_solve(cuda, n, nbw):
     import torch
     import cuev_b200 as cv

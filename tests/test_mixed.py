@@ -57,7 +57,7 @@ def test_refine_int8_products_from_fp32_start(cuda, n):
     assert np.array_equal(dA.cpu().numpy().T, A)   # A is not modified
 
 
-@pytest.mark.parametrize("n", [1024, 4096])
+@pytest.mark.parametrize("n", [2, 20, 100, 1024, 4096])
 def test_mixed_solve_vs_lapack(cuda, n):
     A = _sym(n, 7 * n)
     w_ref = np.linalg.eigvalsh(A)

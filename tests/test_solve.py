@@ -35,7 +35,8 @@ def _sym(n, seed):
                                       (2, 64, 128), (3, 64, 128), (40, 64, 128), (65, 64, 128),
                                       (100, 64, 128), (130, 64, 128), (20, 32, 128),
                                       (31, 32, 128), (32, 32, 128), (63, 64, 128), (64, 64, 128),
-                                      (2048, 0, 0)])
+                                      (64, 32, 128), (96, 32, 128), (128, 64, 128),
+                                      (300, 32, 32), (300, 64, 64), (2048, 0, 0)])
 def test_solve_vs_dsyevd(cuda, n, nbw, nk):
     A = _sym(n, n + nbw)
     w, V = _solve(cuda, A, nbw, nk)
@@ -232,7 +233,7 @@ def test_timer_and_reuse(cuda):
     assert d["total_ms"] >= d["dbbr_ms"]
 
 
-@pytest.mark.parametrize("n", [300, 3072])
+@pytest.mark.parametrize("n", [2, 20, 33, 65, 300, 3072])
 def test_fp32_entry(cuda, n):
     """symm_eig_solve<float>: BC-back runs in FP32 and, at n = 3072, the back-transform's products
     (>= 2^30 multiply-adds) on the FP32-level int8 tensor-core path; the reference's own FP32
