@@ -55,7 +55,7 @@ def _sym(n, seed, dev):
     return ((G + G.t()) / 2).to(dev)
 
 
-@pytest.mark.parametrize("n", [64, 300, 1024, 4096])
+@pytest.mark.parametrize("n", [2, 5, 33, 64, 300, 1024, 4096])
 def test_adjoint_vs_torch_eigh(cuda, n):
     """Against torch.linalg.eigh's gradient, up to n = 4096 (the differentiation config).  Both
     gradients carry each solver's eigenvector rounding divided by the smallest eigenvalue gaps
