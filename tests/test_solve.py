@@ -295,3 +295,42 @@ def test_error_codes(cuda):
     A2 = _sym(n, 6)
     w2, V2 = _solve(cuda, A2)
     assert np.abs(w2 - np.linalg.eigvalsh(A2)).max() < 1e-12 * np.abs(w2).max()
+
+
+def test_concurrent_solves_on_two_threads(cuda):
+    """Two host threads, each with its own stream, solve different matrices at the same time (one
+    finds the cached workspace busy and takes its own), three rounds; every result must match
+    LAPACK."""
+    import threading
+    import torch
+    import cuev_b200 as cv
+    jobs = [(777, 32, 128), (1000, 64, 256)]
+    mats = {n: _sym(n, 40 + n) for n, _, _ in jobs}
+    refs = {n: sla.eigh(mats[n], eigvals_only=True, driver="evd") for n in mats}
+    errors = []
+
+    def worker(n, nbw, nk):
+        try:
+            s = torch.cuda.Stream()
+            with torch.cuda.stream(s):
+                for _ in range(3):
+                    A = mats[n]
+                    dA = torch.from_numpy(np.asfortranarray(A).ravel(order="F").copy()).to(cuda)
+                    w = torch.zeros(n, dtype=torch.float64, device=cuda)
+                    V = torch.zeros(n * n, dtype=torch.float64, device=cuda)
+                    cv.symm_eig_solve(dA, n, w, V, stream=s, nbw=nbw, nk=nk)
+                    s.synchronize()
+                    wn = w.cpu().numpy()
+                    Vn = V.cpu().numpy().reshape((n, n)).T
+                    m = O.metrics(A, wn, Vn, refs[n])
+                    if not (m["max_dlambda_rel"] < 1e-12 and m["resid_n_norm2"] < 1e-13):
+                        errors.append((n, m))
+        except Exception as exc:  # reported below, on the main thread
+            errors.append((n, repr(exc)))
+
+    threads = [threading.Thread(target=worker, args=job) for job in jobs]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert not errors, errors
